@@ -1,0 +1,520 @@
+#!/usr/bin/env python
+"""Benchmark: survey xi_ell / P_ell jobs per second at 512^3 on one B200.
+
+Workload (the precision-form configuration): a survey sector (RA, Dec in
+[-30, 30] deg about +x, r in [500, 1500] Mpc/h, observer at the origin),
+20M clustered data points (1e4 Gaussian clumps, sigma 5 Mpc/h) and 100M
+uniform randoms, weights U[0.5, 1.5], TSC mass assignment on a 512^3 grid,
+ell = 0, 2, 4, xi_ell with rmax 200 / dr 5 and P_ell with kmax 0.3 / dk 0.005.
+
+One step = one survey job: assign D and R' = -alpha R (alpha = sum wD / sum wR)
+into two device grids, form NN = D + R' on the device, run the Y_lm
+correlator on NN and on RR = R', fetch both histogram tables and solve the
+SE15 boundary correction (compute_xi) on the host.  `value` is jobs/s of the
+FP32-mixed form with the catalogs already resident in HBM; `e2e` is the same
+job through the C ABI from pinned host buffers (host->device copies and the
+result readback inside the timed region); `fp64_gpu` is the plain FP64 GPU
+form on the same inputs.  Inputs are GBs, far larger than the 126 MB L2, so
+no explicit L2 flush is needed between steps.
+
+`--impl reference` times the reference's own C++ (compiled from its sources
+with the project FFT shim, OpenMP, all host threads) on a bounded sample of
+the same job and reports the extrapolated jobs/s.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "xi_ell/P_ell survey jobs/s at 512^3, ell<=4 (FP32-mixed; FP64 GPU alongside)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ngrid", type=int, default=512)
+    ap.add_argument("--nd", type=float, default=20e6)
+    ap.add_argument("--nr", type=float, default=100e6)
+    ap.add_argument("--maxell", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------ environment
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Barrier and max-reduction across ranks (gloo; no data-path traffic)."""
+
+    def __init__(self, world):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ job
+
+class Workload:
+    def __init__(self, a):
+        from fftcorr_b200 import mocks
+        self.ngrid = (a.ngrid,) * 3
+        self.nd = int(a.nd)
+        self.nr = int(a.nr)
+        self.maxell = a.maxell
+        self.rmax, self.dr = 200.0, 5.0
+        self.kmax, self.dk = 0.3, 0.005
+        self.sector = mocks.Sector()
+        self.posmin, self.cell = mocks.survey_box(self.sector, self.rmax, self.ngrid)
+
+    def describe(self):
+        return {"workload": "survey xi_ell+P_ell job: sector r 500-1500 Mpc/h, "
+                            "RA/Dec +-30 deg, clustered data + uniform randoms",
+                "grid": list(self.ngrid), "n_data": self.nd, "n_randoms": self.nr,
+                "scheme": "TSC", "maxell": self.maxell, "rmax": self.rmax,
+                "dr": self.dr, "kmax": self.kmax, "dk": self.dk,
+                "cell_size": round(self.cell, 6),
+                "l2": "inputs and grids are GBs (> 126 MB L2); no flush needed"}
+
+    def catalogs(self, seed_offset=0):
+        from fftcorr_b200 import mocks
+        D = mocks.sector_clustered(self.nd, 2 + 100 * seed_offset, sector=self.sector)
+        R = mocks.sector_randoms(self.nr, 3 + 100 * seed_offset, sector=self.sector)
+        R[:, 3] *= -(D[:, 3].sum() / R[:, 3].sum())
+        return D, R
+
+
+class SurveyJob:
+    """Device objects for one survey job, reused across steps."""
+
+    def __init__(self, w, precision):
+        import fftcorr_b200 as fb
+        from fftcorr_b200.correlate import TSC_ALIASED_CORRECTION
+        self.fb = fb
+        self.w = w
+        self.gA = fb.ConfigSpaceGrid.from_geometry(w.ngrid, w.posmin, w.cell)
+        self.gB = fb.ConfigSpaceGrid.from_geometry(w.ngrid, w.posmin, w.cell)
+        tsc = fb.DistributionScheme.TRIANGULAR_SHAPED_CLOUD
+        self.maA = fb.MassAssignor(self.gA, tsc, False, 0)
+        self.maB = fb.MassAssignor(self.gB, tsc, False, 0)
+        self.corr = fb.Correlator(w.ngrid, w.cell, w.posmin, TSC_ALIASED_CORRECTION,
+                                  w.rmax, w.dr, w.kmax, w.dk, w.maxell,
+                                  precision=precision)
+
+    def _reset(self):
+        from fftcorr_b200 import _lib
+        _lib.call("fc_grid_clear", self.gA.handle)
+        _lib.call("fc_grid_clear", self.gB.handle)
+        self.maA.clear()
+        self.maB.clear()
+
+    def _correlate(self):
+        from fftcorr_b200.correlate import compute_xi
+        self.corr.autocorrelate(self.gA)
+        nn = self.corr.results()
+        self.corr.autocorrelate(self.gB)
+        rr = self.corr.results()
+        xi = compute_xi(nn["rhist"].T, rr["rhist"].T)
+        return nn, rr, xi
+
+    def run_device(self, dD, nD, dR, nR):
+        self._reset()
+        self.maA.add_particles_device(dD, nD)
+        self.maB.add_particles_device(dR, nR)
+        self.gA.add_grid(self.gB)
+        return self._correlate()
+
+    def run_host(self, D, R):
+        self._reset()
+        self.maA.add_particles(D)
+        self.maB.add_particles(R)
+        self.gA.add_grid(self.gB)
+        return self._correlate()
+
+    def result_bytes(self, nn):
+        per = sum(np.asarray(v).nbytes for k, v in nn.items() if k != "zerolag") + 8
+        return 2 * per
+
+
+def device_copy(arr):
+    from fftcorr_b200 import _lib
+    p = ctypes.c_void_p()
+    _lib.call("fc_device_malloc", arr.nbytes, ctypes.byref(p))
+    _lib.call("fc_memcpy_htod", p, arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes)
+    return p.value
+
+
+class DeviceTimer:
+    def __init__(self):
+        from fftcorr_b200 import _lib
+        self._lib = _lib
+        self.h = ctypes.c_void_p()
+        _lib.call("fc_timer_create", ctypes.byref(self.h))
+
+    def start(self):
+        self._lib.call("fc_timer_start", self.h)
+
+    def stop(self):
+        s = ctypes.c_double()
+        self._lib.call("fc_timer_stop", self.h, ctypes.byref(s))
+        return s.value
+
+
+def kernel_profile(job, dD, nD, dR, nR):
+    """Per-kernel-family device time of one job with profiling on."""
+    from fftcorr_b200 import _lib
+    _lib.call("fc_corr_set_profiling", job.corr.handle, 1)
+    job.run_device(dD, nD, dR, nR)
+    arr = (_lib.KernelTime * 32)()
+    n = ctypes.c_int()
+    _lib.call("fc_corr_profile", job.corr.handle, arr, 32, ctypes.byref(n))
+    _lib.call("fc_corr_set_profiling", job.corr.handle, 0)
+    out = {}
+    for i in range(n.value):
+        out[arr[i].name.decode()] = {"launches": arr[i].launches,
+                                     "seconds": arr[i].seconds}
+    return out
+
+
+def algorithmic_bytes(family, w, precision):
+    """Bytes one launch must move at minimum (read + write once)."""
+    s = 8 if precision == "fp64" else 4
+    n = w.ngrid[0] * w.ngrid[1] * w.ngrid[2]
+    nc = w.ngrid[0] * w.ngrid[1] * (w.ngrid[2] // 2 + 1)
+    table = {
+        "weight": n * 8 + n * s,          # rho FP64 in, Y_lm*rho out
+        "copy_pad": n * 8 + n * s,
+        "conj_mul": 3 * nc * 2 * s,       # F in, G in, F*conj(G) out
+        "r2c": n * s + nc * 2 * s,
+        "c2r": nc * 2 * s + n * s,
+    }
+    return table.get(family)
+
+
+# --------------------------------------------------------- CPU baseline
+
+def cpu_baseline_sample(w, R, threads):
+    """Times the reference C++ (OpenMP build) on a bounded sample and
+    extrapolates to one job.  Returns (jobs_per_s, description)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libfcref_omp.so")
+    if not os.path.exists(lib_path):
+        return None, "oracle/_ref/libfcref_omp.so missing"
+    L = ctypes.CDLL(lib_path)
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))  # noqa: E731
+    nsample = min(10_000_000, R.shape[0])
+    sample = np.ascontiguousarray(R[:nsample])
+    shape = np.array(w.ngrid, dtype=np.intc)
+    grid = np.zeros(w.ngrid)
+    st = np.zeros(6)
+    t0 = time.perf_counter()
+    rc = L.fcref_mass_assign(dp(sample), ctypes.c_long(nsample), ip(shape),
+                             dp(np.asarray(w.posmin, dtype=np.float64)),
+                             ctypes.c_double(w.cell), 1, 0, ctypes.c_long(1000000),
+                             dp(grid), dp(st), 1)
+    t_ma = time.perf_counter() - t0
+    if rc != 0:
+        return None, "reference mass assignment failed"
+    nrows = 1
+    nr = int(math.floor(w.rmax / w.dr))
+    nk = int(math.floor(w.kmax / w.dk))
+    bufs = [np.zeros(nr), np.zeros((nrows, nr), dtype=np.intc), np.zeros((nrows, nr)),
+            np.zeros(nk), np.zeros((nrows, nk), dtype=np.intc), np.zeros((nrows, nk))]
+    zl = ctypes.c_double()
+    timers = np.zeros(8)
+    t0 = time.perf_counter()
+    rc = L.fcref_correlate(
+        1, dp(grid), None, ip(shape), ctypes.c_double(w.cell),
+        dp(np.asarray(w.posmin, dtype=np.float64)), 2, ctypes.c_double(w.rmax),
+        ctypes.c_double(w.dr), ctypes.c_double(w.kmax), ctypes.c_double(w.dk), 0,
+        dp(bufs[0]), ip(bufs[1]), dp(bufs[2]), dp(bufs[3]), ip(bufs[4]), dp(bufs[5]),
+        ctypes.byref(zl), 1, dp(timers))
+    t_corr = time.perf_counter() - t0
+    if rc != 0:
+        return None, "reference correlation failed"
+    setup, _, fft, extract, mult, ylm, hist, total = timers
+    t_fft = fft / 4.0   # ell_max = 0: grid2, the reference's extra grid1, r2c, c2r
+    t_lm = 2 * t_fft + ylm + mult + extract + hist
+    n_lm = sum(2 * l + 1 for l in range(0, w.maxell + 1, 2))
+    corr_job = setup + total + (n_lm - 1) * t_lm
+    # The reference CLI flow assigns D+R' for NN and R' again for RR.
+    ma_job = t_ma * (2 * w.nr + w.nd) / nsample
+    job = ma_job + 2 * corr_job
+    desc = (f"reference C++ (cc/, OpenMP -DFFTSLAB, project FFT shim; FFTW "
+            f"unavailable) on {threads} threads: MassAssignor on {nsample} of the "
+            f"randoms (buffer 1e6) scaled to {2 * w.nr + w.nd} assignments, plus "
+            f"one Correlator run at {w.ngrid[0]}^3 with ell_max=0 timed by the "
+            f"reference's own timers and extrapolated to {n_lm} (ell,m) terms; "
+            f"sample wall {t_ma + t_corr:.1f} s")
+    return 1.0 / job, desc
+
+
+# ------------------------------------------------------------------ main
+
+def run_reference(a, rank):
+    if rank != 0:
+        return
+    w = Workload(a)
+    threads = os.cpu_count() or 1
+    from fftcorr_b200 import mocks
+    R = mocks.sector_randoms(min(int(a.nr), 10_000_000), 3, sector=w.sector)
+    R[:, 3] *= -1.0
+    vals = []
+    desc = ""
+    for i in range(a.warmup + a.steps):
+        v, desc = cpu_baseline_sample(w, R, threads)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": desc}))
+            return
+        if i >= a.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "jobs/s",
+        "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": w.describe(),
+        "cpu_baseline": {"value": value, "unit": "jobs/s", "cores": threads,
+                         "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": "jobs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_env()
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+    from fftcorr_b200 import _lib
+    _lib.call("fc_set_device", local)
+    dist = Dist(world)
+    w = Workload(a)
+    t_gen = time.perf_counter()
+    D, R = w.catalogs(seed_offset=rank)
+    t_gen = time.perf_counter() - t_gen
+    nD, nR = D.shape[0], R.shape[0]
+    for arr in (D, R):
+        _lib.call("fc_host_register", arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes)
+    dD, dR = device_copy(D), device_copy(R)
+    timer = DeviceTimer()
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        dist.barrier()
+        timer.start()
+        for _ in range(steps):
+            out = fn()
+        secs = timer.stop()
+        return dist.max(secs), out
+
+    # FP32-mixed form: device-resident inputs, then end to end from host.
+    job = SurveyJob(w, "fp32")
+    with ClockSampler(local) as clocks:
+        t_dev, (nn, rr, xi) = timed(lambda: job.run_device(dD, nD, dR, nR),
+                                    a.steps, a.warmup)
+    t_e2e, _ = timed(lambda: job.run_host(D, R), a.steps, 1)
+    prof = kernel_profile(job, dD, nD, dR, nR)
+    ma_stats = job.maB._stats()
+    res32 = (nn, rr, xi)
+    result_bytes = job.result_bytes(nn)
+    del job
+
+    fp64 = None
+    if not a.no_fp64:
+        job64 = SurveyJob(w, "fp64")
+        t64, (nn64, rr64, xi64) = timed(lambda: job64.run_device(dD, nD, dR, nR),
+                                        a.steps, 1)
+        prof64 = kernel_profile(job64, dD, nD, dR, nR)
+        del job64
+        # Largest deviation of every FP32-mixed multipole from the FP64 run,
+        # relative to the rms of its monopole.
+        def maxdev(a32, a64):
+            rms0 = float(np.sqrt(np.mean(a64[:, 0] ** 2)))
+            return [float(np.max(np.abs(a32[:, l] - a64[:, l])) / rms0)
+                    for l in range(a64.shape[1])]
+        fp64 = {
+            "value": world * a.steps / t64, "unit": "jobs/s",
+            "ms_per_step": 1000.0 * t64 / a.steps,
+            "fp32_vs_fp64_xi_maxdev_over_rms_xi0": maxdev(xi, xi64),
+            "fp32_vs_fp64_NN_maxdev_over_rms_0": maxdev(nn["rhist"].T, nn64["rhist"].T),
+            "fp32_vs_fp64_P_maxdev_over_rms_P0": maxdev(nn["khist"].T, nn64["khist"].T),
+            "kernels": prof64,
+        }
+
+    value = world * a.steps / t_dev
+    e2e_value = world * a.steps / t_e2e
+    peak, peak_kind = measured_hbm_peak()
+    # Roofline of the dominant hand-written kernel (cuFFT's are listed too).
+    roof = None
+    ours = {k: v for k, v in prof.items() if k not in ("r2c", "c2r")}
+    if ours:
+        fam = max(ours, key=lambda k: ours[k]["seconds"])
+        per = ours[fam]["seconds"] / max(1, ours[fam]["launches"])
+        alg = algorithmic_bytes(fam, w, "fp32")
+        if alg:
+            achieved = alg / per / 1e9
+            roof = {"kernel": fam, "bound": "hbm", "achieved": achieved, "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                    "bytes_per_launch": alg, "us_per_launch": per * 1e6,
+                    "traffic": None}
+    fft_roof = {}
+    for fam in ("r2c", "c2r"):
+        if fam in prof:
+            per = prof[fam]["seconds"] / max(1, prof[fam]["launches"])
+            alg = algorithmic_bytes(fam, w, "fp32")
+            fft_roof[fam] = {"achieved": alg / per / 1e9, "frac": alg / per / 1e9 / peak,
+                             "us_per_launch": per * 1e6}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cv, desc = cpu_baseline_sample(w, R, threads)
+        if cv is not None:
+            cpu = {"value": cv, "unit": "jobs/s", "cores": threads,
+                   "kind": "reference", "sample": desc}
+
+    gpu_launches = sum(v["launches"] for k, v in prof.items() if k not in ("r2c", "c2r"))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "jobs/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1000.0 * t_dev / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded mock survey catalogs, see config)",
+            "config": dict(w.describe(), parallelism=f"replicas x{world}",
+                           form="fp32-mixed, inputs resident in HBM"),
+            "e2e": {"value": e2e_value, "unit": "jobs/s",
+                    "h2d_bytes_per_step": int(D.nbytes + R.nbytes),
+                    "d2h_bytes_per_step": int(result_bytes),
+                    "ms_per_step": 1000.0 * t_e2e / a.steps},
+            "fp64_gpu": fp64,
+            "roofline": roof,
+            "fft_roofline": fft_roof,
+            "kernels": prof,
+            "mass_assign_s_per_flush": {"sort": ma_stats.sort_time,
+                                        "scatter": ma_stats.window_time},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "gpu_launches": gpu_launches,
+            "catalog_generation_s": t_gen,
+        }
+        print(json.dumps(line))
+    for p in (dD, dR):
+        _lib.call("fc_device_free", ctypes.c_void_p(p))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

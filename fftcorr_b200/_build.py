@@ -1,0 +1,110 @@
+"""Builds the fftcorr_b200 CUDA library in-tree for sm_100a.
+
+    python -m fftcorr_b200._build [--reference DIR]
+
+Outputs fftcorr_b200/libfftcorr_b200.so (git-ignored; it travels with the
+source tree).  When the reference source tree is available its D12 wavelet
+table is generated into csrc/_gen/ first (see csrc/gen_d12.cc); without it
+the library is built without the D12 scheme and reports FC_ERR_UNSUPPORTED
+for it.
+"""
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+GEN = os.path.join(CSRC, "_gen")
+LIB = os.path.join(HERE, "libfftcorr_b200.so")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+DEFAULT_REFERENCE = "/root/reference"
+
+SOURCES = ["fc_core.cu", "fc_hist.cu", "fc_assign.cu", "fc_corr.cu"]
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    # Products are rounded one by one like the reference's FP64 code.
+    "-fmad=false",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+    "--expt-relaxed-constexpr",
+]
+
+
+def _run(cmd, cwd=None):
+    print("+", " ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=cwd)
+
+
+def generate_d12(reference):
+    """Writes csrc/_gen/d12_table.inc from the reference's d12.h, if present."""
+    header = os.path.join(reference, "cc", "particle_mesh", "d12.h")
+    out = os.path.join(GEN, "d12_table.inc")
+    if not os.path.exists(header):
+        return os.path.exists(out)
+    os.makedirs(GEN, exist_ok=True)
+    exe = os.path.join(GEN, "gen_d12")
+    _run(["g++", "-std=c++11", "-O0", "-I", os.path.join(reference, "cc"),
+          os.path.join(CSRC, "gen_d12.cc"), "-o", exe])
+    table = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    tmp = out + ".tmp"
+    with open(tmp, "w") as f:
+        f.write(table)
+    os.replace(tmp, out)
+    return True
+
+
+def sources():
+    return [os.path.join(CSRC, s) for s in SOURCES]
+
+
+def needs_rebuild():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+                        if f.endswith((".cuh", ".h"))]
+    deps.append(os.path.join(HERE, "..", "include", "fc_api.h"))
+    gen = os.path.join(GEN, "d12_table.inc")
+    if os.path.exists(gen):
+        deps.append(gen)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(reference=DEFAULT_REFERENCE, force=False, verbose_ptxas=False):
+    generate_d12(reference)
+    if not force and not needs_rebuild():
+        return LIB
+    if not os.path.exists(NVCC):
+        raise RuntimeError(f"nvcc not found at {NVCC}")
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        _run([NVCC, *NVCC_FLAGS, *extra, "-I", CSRC, "-c",
+              src, "-o", obj])
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+          *objs, "-o", tmp, "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft",
+          "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")])
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=DEFAULT_REFERENCE)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas-v", action="store_true")
+    a = ap.parse_args(argv)
+    print(build(a.reference, a.force, a.ptxas_v))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,381 @@
+// fc_core.cu -- error state, device selection, ConfigSpaceGrid and the
+// array_ops reductions of the fftcorr_b200 library.
+//
+// ConfigSpaceGrid mirrors cc/grid/config_space_grid.h:10-57 with the grid in
+// HBM; sum/sumsq/add_scalar/multiply_by mirror cc/array/array_ops.cc:55-137.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "fc_common.cuh"
+#include "fc_internal.h"
+
+namespace fc {
+
+namespace {
+thread_local std::string t_last_error;
+}
+
+void set_last_error(const std::string &msg) { t_last_error = msg; }
+
+const char *last_error_cstr() { return t_last_error.c_str(); }
+
+int sm_count() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int cached[64] = {0};
+  if (dev >= 0 && dev < 64 && cached[dev]) return cached[dev];
+  int n = 148;
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+      cudaSuccess)
+    n = 148;
+  if (dev >= 0 && dev < 64) cached[dev] = n;
+  return n;
+}
+
+YlmParams make_ylm_params(int ell, int m, double coeff) {
+  // spherical_harmonics.h:36-38 validity checks.
+  if (!(ell == 0 || ell == 2 || ell == 4))
+    FC_THROW(FC_ERR_INVALID, "Unsupported ell");
+  if (m < -ell || m > ell) FC_THROW(FC_ERR_INVALID, "Illegal (ell, m)");
+  YlmParams p;
+  p.ell = ell;
+  p.m = m;
+  // spherical_harmonics.h:52 (ell = 0 shortcut) and :85-87.
+  p.value0 = coeff / sqrt(4.0 * M_PI);
+  double isqpi = sqrt(1.0 / M_PI);
+  isqpi *= coeff;
+  if (m != 0) isqpi *= sqrt(2.0);
+  p.isqpi = isqpi;
+  return p;
+}
+
+// --------------------------------------------------------------- kernels
+
+namespace {
+
+__global__ void k_fill(double *a, size_t n, double v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] = v;
+}
+
+__global__ void k_add_scalar(double *a, size_t n, double s) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] += s;
+}
+
+__global__ void k_multiply_by(double *a, size_t n, double s) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    a[i] *= s;
+}
+
+__global__ void k_axpy(double *y, const double *x, size_t n, double a) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+
+// Pass 1 of the deterministic sum/sumsq: block b reduces the grid-stride
+// subsequence it owns in a fixed order.
+__global__ void k_sum_partials(const double *a, size_t n, double *partials) {
+  __shared__ double red[32];
+  double s = 0.0, q = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double v = a[i];
+    s += v;
+    q += v * v;
+  }
+  s = block_sum(s, red);
+  q = block_sum(q, red);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = s;
+    partials[2 * blockIdx.x + 1] = q;
+  }
+}
+
+// Pass 2: one block folds the partials in block order.
+__global__ void k_sum_final(const double *partials, int nparts, double *out) {
+  __shared__ double red[32];
+  double s = 0.0, q = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    s += partials[2 * i];
+    q += partials[2 * i + 1];
+  }
+  s = block_sum(s, red);
+  q = block_sum(q, red);
+  if (threadIdx.x == 0) {
+    out[0] = s;
+    out[1] = q;
+  }
+}
+
+}  // namespace
+
+void device_fill(double *a, size_t n, double v, cudaStream_t s) {
+  if (n == 0) return;
+  k_fill<<<grid_for(n, 256), 256, 0, s>>>(a, n, v);
+  FC_LAUNCH_CHECK();
+}
+
+void device_sum_sumsq(const double *a, size_t n, double *scratch,
+                      cudaStream_t s) {
+  // scratch: 2 * kSumBlocks partials followed by the 2 results.
+  k_sum_partials<<<kSumBlocks, 256, 0, s>>>(a, n, scratch);
+  FC_LAUNCH_CHECK();
+  k_sum_final<<<1, 256, 0, s>>>(scratch, kSumBlocks, scratch + 2 * kSumBlocks);
+  FC_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------- the grid
+
+Grid::Grid(const int shp[3], const double pmin[3], double cell) {
+  for (int i = 0; i < 3; ++i) {
+    FC_REQUIRE(shp[i] > 0, FC_ERR_INVALID, "grid shape must be positive");
+    shape[i] = shp[i];
+    posmin[i] = pmin[i];
+  }
+  FC_REQUIRE(cell > 0, FC_ERR_INVALID, "cell_size must be positive");
+  cell_size = cell;
+  FC_CUDA(cudaGetDevice(&device));
+  FC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  data.resize(size() * sizeof(double));
+  scratch.resize((2 * kSumBlocks + 2) * sizeof(double));
+  clear();
+}
+
+Grid::~Grid() {
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
+}
+
+void Grid::clear() {
+  FC_CUDA(cudaMemsetAsync(data.get(), 0, size() * sizeof(double), stream));
+}
+
+}  // namespace fc
+
+// ============================================================== C entry
+
+using namespace fc;
+
+extern "C" {
+
+const char *fc_last_error(void) { return fc::last_error_cstr(); }
+
+int fc_version(void) { return 10000 * 0 + 100 * 9 + 0; }
+
+int fc_set_device(int device) {
+  return guard([&] { FC_CUDA(cudaSetDevice(device)); });
+}
+
+int fc_grid_create(const int shape[3], const double posmin[3],
+                   double cell_size, fc_grid **out) {
+  return guard([&] {
+    FC_REQUIRE(shape && posmin && out, FC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    Grid *g = new Grid(shape, posmin, cell_size);
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+    *out = reinterpret_cast<fc_grid *>(g);
+  });
+}
+
+int fc_grid_destroy(fc_grid *grid) {
+  return guard([&] { delete reinterpret_cast<Grid *>(grid); });
+}
+
+int fc_grid_clear(fc_grid *grid) {
+  return guard([&] {
+    Grid *g = as_grid(grid);
+    g->clear();
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+  });
+}
+
+int fc_grid_upload(fc_grid *grid, const double *host) {
+  return guard([&] {
+    Grid *g = as_grid(grid);
+    FC_REQUIRE(host, FC_ERR_INVALID, "null host pointer");
+    FC_CUDA(cudaMemcpyAsync(g->ptr(), host, g->size() * sizeof(double),
+                            cudaMemcpyHostToDevice, g->stream));
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+  });
+}
+
+int fc_grid_download(const fc_grid *grid, double *host) {
+  return guard([&] {
+    const Grid *g = as_grid(grid);
+    FC_REQUIRE(host, FC_ERR_INVALID, "null host pointer");
+    FC_CUDA(cudaMemcpyAsync(host, g->ptr(), g->size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, g->stream));
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+  });
+}
+
+int fc_grid_device_ptr(const fc_grid *grid, double **device_ptr) {
+  return guard([&] {
+    FC_REQUIRE(device_ptr, FC_ERR_INVALID, "null argument");
+    *device_ptr = as_grid(grid)->ptr();
+  });
+}
+
+int fc_grid_coords(const fc_grid *grid, const double survey[3], int periodic,
+                   double grid_coords[3], int *inside) {
+  return guard([&] {
+    const Grid *g = as_grid(grid);
+    FC_REQUIRE(survey && grid_coords && inside, FC_ERR_INVALID,
+               "null argument");
+    *inside = host_grid_coords(survey, g->posmin, g->cell_size, g->shape,
+                               periodic != 0, grid_coords)
+                  ? 1
+                  : 0;
+  });
+}
+
+int fc_grid_sum(fc_grid *grid, double *sum, double *sumsq) {
+  return guard([&] {
+    Grid *g = as_grid(grid);
+    double *scr = g->scratch.as<double>();
+    device_sum_sumsq(g->ptr(), g->size(), scr, g->stream);
+    double res[2];
+    FC_CUDA(cudaMemcpyAsync(res, scr + 2 * kSumBlocks, sizeof(res),
+                            cudaMemcpyDeviceToHost, g->stream));
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+    if (sum) *sum = res[0];
+    if (sumsq) *sumsq = res[1];
+  });
+}
+
+int fc_grid_add_scalar(fc_grid *grid, double s) {
+  return guard([&] {
+    Grid *g = as_grid(grid);
+    k_add_scalar<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
+        g->ptr(), g->size(), s);
+    FC_LAUNCH_CHECK();
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+  });
+}
+
+int fc_grid_multiply_by(fc_grid *grid, double s) {
+  return guard([&] {
+    Grid *g = as_grid(grid);
+    k_multiply_by<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
+        g->ptr(), g->size(), s);
+    FC_LAUNCH_CHECK();
+    FC_CUDA(cudaStreamSynchronize(g->stream));
+  });
+}
+
+int fc_grid_axpy(fc_grid *y, double a, const fc_grid *x) {
+  return guard([&] {
+    Grid *gy = as_grid(y);
+    const Grid *gx = as_grid(x);
+    for (int i = 0; i < 3; ++i)
+      FC_REQUIRE(gy->shape[i] == gx->shape[i], FC_ERR_INVALID,
+                 "Incompatible shapes for axpy.");
+    // Order after any pending work on x's stream.
+    cudaEvent_t ev;
+    FC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaEventRecord(ev, gx->stream);
+    cudaStreamWaitEvent(gy->stream, ev, 0);
+    cudaEventDestroy(ev);
+    k_axpy<<<grid_for(gy->size(), 256), 256, 0, gy->stream>>>(
+        gy->ptr(), gx->ptr(), gy->size(), a);
+    FC_LAUNCH_CHECK();
+    FC_CUDA(cudaStreamSynchronize(gy->stream));
+  });
+}
+
+}  // extern "C"
+
+// ============================================================ utilities
+
+namespace {
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+}  // namespace
+
+extern "C" {
+
+int fc_device_synchronize(void) {
+  return guard([&] { FC_CUDA(cudaDeviceSynchronize()); });
+}
+
+int fc_host_register(void *ptr, size_t bytes) {
+  return guard([&] {
+    FC_REQUIRE(ptr, FC_ERR_INVALID, "null pointer");
+    FC_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  });
+}
+
+int fc_host_unregister(void *ptr) {
+  return guard([&] { FC_CUDA(cudaHostUnregister(ptr)); });
+}
+
+int fc_device_malloc(size_t bytes, void **ptr) {
+  return guard([&] {
+    FC_REQUIRE(ptr, FC_ERR_INVALID, "null pointer");
+    *ptr = nullptr;
+    FC_CUDA(cudaMalloc(ptr, bytes));
+  });
+}
+
+int fc_device_free(void *ptr) {
+  return guard([&] { FC_CUDA(cudaFree(ptr)); });
+}
+
+int fc_memcpy_htod(void *dst, const void *src, size_t bytes) {
+  return guard([&] {
+    FC_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  });
+}
+
+int fc_timer_create(fc_timer **t) {
+  return guard([&] {
+    FC_REQUIRE(t, FC_ERR_INVALID, "null pointer");
+    Timer *x = new Timer;
+    FC_CUDA(cudaEventCreate(&x->a));
+    FC_CUDA(cudaEventCreate(&x->b));
+    *t = reinterpret_cast<fc_timer *>(x);
+  });
+}
+
+int fc_timer_start(fc_timer *t) {
+  return guard([&] {
+    FC_REQUIRE(t, FC_ERR_INVALID, "null timer");
+    Timer *x = reinterpret_cast<Timer *>(t);
+    FC_CUDA(cudaDeviceSynchronize());
+    FC_CUDA(cudaEventRecord(x->a, 0));
+  });
+}
+
+int fc_timer_stop(fc_timer *t, double *seconds) {
+  return guard([&] {
+    FC_REQUIRE(t && seconds, FC_ERR_INVALID, "null argument");
+    Timer *x = reinterpret_cast<Timer *>(t);
+    FC_CUDA(cudaDeviceSynchronize());
+    FC_CUDA(cudaEventRecord(x->b, 0));
+    FC_CUDA(cudaEventSynchronize(x->b));
+    float ms = 0.f;
+    FC_CUDA(cudaEventElapsedTime(&ms, x->a, x->b));
+    *seconds = ms * 1e-3;
+  });
+}
+
+int fc_timer_destroy(fc_timer *t) {
+  return guard([&] {
+    Timer *x = reinterpret_cast<Timer *>(t);
+    if (!x) return;
+    if (x->a) cudaEventDestroy(x->a);
+    if (x->b) cudaEventDestroy(x->b);
+    delete x;
+  });
+}
+
+}  // extern "C"

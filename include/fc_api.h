@@ -1,0 +1,257 @@
+/*
+ * fc_api.h -- C ABI of the fftcorr_b200 library (B200 / sm_100a).
+ *
+ * This is the drop-in boundary behind the reference fftcorr API.  Every
+ * entry point is `extern "C"`, takes plain pointers and sizes, and returns an
+ * fc_status (0 on success, a negative code otherwise; fc_last_error() gives
+ * the message).  Host pointers are borrowed for the duration of the call.
+ * Device memory is owned by the opaque handles.  Calls are synchronous
+ * unless their name ends in _async; handles are not thread-safe (like the
+ * reference classes), distinct handles may be used from distinct threads.
+ *
+ * Reference interfaces replaced (file:line in cshallue/fftcorr):
+ *   ConfigSpaceGrid    cc/grid/config_space_grid.h:10-57,
+ *                      fftcorr/grid/config_space_grid.pxd:9-14
+ *   MassAssignor       cc/particle_mesh/mass_assignor.h:30-234,
+ *                      fftcorr/particle_mesh/mass_assignor.pxd:10-29
+ *   DistributionScheme cc/particle_mesh/distribution_functions.h:11-15
+ *   PeriodicCorrelator cc/correlate/correlator.h:254-358
+ *   Correlator         cc/correlate/correlator.h:360-505,
+ *                      fftcorr/correlate/correlator.pxd:21-66
+ *   WindowCorrection   cc/correlate/window_correct.h:8-12
+ *   HistogramList      cc/histogram/histogram_list.h:10-68,
+ *                      fftcorr/histogram/histogram_list.pxd:6-13
+ *   array_ops sum/sumsq/add_scalar/multiply_by  cc/array/array_ops.h:16-20
+ */
+#ifndef FC_API_H
+#define FC_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef enum fc_status {
+  FC_OK = 0,
+  FC_ERR_INVALID = -1,     /* std::invalid_argument in the reference     */
+  FC_ERR_RANGE = -2,       /* std::out_of_range                           */
+  FC_ERR_ALLOC = -3,       /* std::bad_alloc (device or pinned host)      */
+  FC_ERR_CUDA = -4,        /* CUDA runtime failure                        */
+  FC_ERR_CUFFT = -5,       /* cuFFT plan or execution failure             */
+  FC_ERR_STATE = -6,       /* std::logic_error: call out of order         */
+  FC_ERR_UNSUPPORTED = -7, /* feature not built into this library         */
+  FC_ERR_TIMEOUT = -8,     /* a bounded device wait gave up               */
+  FC_ERR_ADMISSION = -9    /* a request does not fit the memory budget    */
+} fc_status;
+
+/* Message of the last failing call on this thread (never NULL). */
+const char *fc_last_error(void);
+/* Library version as 10000*major + 100*minor + patch. */
+int fc_version(void);
+/* Selects the CUDA device used by handles created afterwards on this thread. */
+int fc_set_device(int device);
+
+/* ------------------------------------------------------------- constants */
+/* DistributionScheme (distribution_functions.h:11-15); 3 is new: trilinear
+ * cloud-in-cell, which the reference does not have. */
+enum {
+  FC_NEAREST_CELL = 0,
+  FC_TRIANGULAR_SHAPED_CLOUD = 1,
+  FC_WAVELET = 2,
+  FC_CLOUD_IN_CELL = 3
+};
+/* WindowCorrection (window_correct.h:8-12). */
+enum {
+  FC_NO_CORRECTION = 0,
+  FC_TSC_CORRECTION = 1,
+  FC_TSC_ALIASED_CORRECTION = 2
+};
+/* Arithmetic of the correlator's grids and FFTs.  FC_FP32_MIXED keeps cell
+ * coordinates, Y_lm normalisation, subgrids and histograms in FP64. */
+enum { FC_FP64 = 0, FC_FP32_MIXED = 1 };
+/* Correlator kinds. */
+enum { FC_PERIODIC = 0, FC_SURVEY = 1 };
+
+/* ------------------------------------------------------- ConfigSpaceGrid */
+typedef struct fc_grid fc_grid;
+
+/* ConfigSpaceGrid(shape, posmin, cell_size): a zeroed FP64 grid in device
+ * memory (config_space_grid.h:12-16). */
+int fc_grid_create(const int shape[3], const double posmin[3],
+                   double cell_size, fc_grid **out);
+int fc_grid_destroy(fc_grid *grid);
+/* ConfigSpaceGrid::clear (config_space_grid.h:27). */
+int fc_grid_clear(fc_grid *grid);
+/* Host <-> device copies of the N0*N1*N2 row-major FP64 grid. */
+int fc_grid_upload(fc_grid *grid, const double *host);
+int fc_grid_download(const fc_grid *grid, double *host);
+/* Device pointer of the grid data (valid until fc_grid_destroy). */
+int fc_grid_device_ptr(const fc_grid *grid, double **device_ptr);
+/* ConfigSpaceGrid::get_grid_coords (config_space_grid.h:31-46); *inside is
+ * set to 1 or 0 like the reference's bool return. */
+int fc_grid_coords(const fc_grid *grid, const double survey[3], int periodic,
+                   double grid_coords[3], int *inside);
+/* array_ops::sum and sumsq (array_ops.cc:95-137), FP64, deterministic. */
+int fc_grid_sum(fc_grid *grid, double *sum, double *sumsq);
+/* array_ops::add_scalar / multiply_by (array_ops.cc:55-93). */
+int fc_grid_add_scalar(fc_grid *grid, double s);
+int fc_grid_multiply_by(fc_grid *grid, double s);
+/* y += a * x elementwise (same shapes).  Used to form N = D - alpha R from
+ * separately assigned catalogs. */
+int fc_grid_axpy(fc_grid *y, double a, const fc_grid *x);
+
+/* ---------------------------------------------------------- MassAssignor */
+typedef struct fc_assignor fc_assignor;
+
+typedef struct fc_assign_stats {
+  uint64_t num_added;
+  uint64_t num_skipped;
+  double totw;
+  double totwsq;
+  double sort_time;   /* seconds, device time of the radix sorts */
+  double window_time; /* seconds, device time of the stencil scatter */
+} fc_assign_stats;
+
+/* MassAssignor(grid, scheme, periodic_wrap, buffer_size)
+ * (mass_assignor.h:32-50).  buffer_size 0 assigns every add call at once;
+ * otherwise particles are buffered on the device and assigned when at least
+ * buffer_size are waiting, or on flush.  The grid must outlive the handle. */
+int fc_assignor_create(fc_grid *grid, int scheme, int periodic_wrap,
+                       int64_t buffer_size, fc_assignor **out);
+int fc_assignor_destroy(fc_assignor *ma);
+/* add_particles_to_buffer overloads (mass_assignor.h:72-103):
+ * posw is (n, 4) x,y,z,w; pos is (n, 3) with weights (n) or one weight. */
+int fc_assignor_add_posw(fc_assignor *ma, const double *posw, int64_t n);
+int fc_assignor_add_pos_weights(fc_assignor *ma, const double *pos,
+                                const double *weights, int64_t n);
+int fc_assignor_add_pos_weight(fc_assignor *ma, const double *pos,
+                               double weight, int64_t n);
+/* Same as fc_assignor_add_posw but posw is already in device memory. */
+int fc_assignor_add_posw_device(fc_assignor *ma, const double *posw_device,
+                                int64_t n);
+/* MassAssignor::flush (mass_assignor.h:127-191). */
+int fc_assignor_flush(fc_assignor *ma);
+/* MassAssignor::clear (mass_assignor.h:60-70). */
+int fc_assignor_clear(fc_assignor *ma);
+int fc_assignor_stats(fc_assignor *ma, fc_assign_stats *stats);
+int fc_assignor_buffer_size(const fc_assignor *ma, int64_t *buffer_size);
+
+/* ------------------------------------------------------------ Correlator */
+typedef struct fc_correlator fc_correlator;
+
+/* PeriodicCorrelator (kind FC_PERIODIC, posmin ignored) or Correlator
+ * (kind FC_SURVEY) (correlator.h:20-39, 366-377).  fft_flags is accepted
+ * for interface compatibility (the reference passes FFTW planner flags). */
+int fc_corr_create(int kind, const int shape[3], double cell_size,
+                   const double posmin[3], int window_correct, double rmax,
+                   double dr, double kmax, double dk, int maxell,
+                   unsigned fft_flags, int precision, fc_correlator **out);
+int fc_corr_destroy(fc_correlator *corr);
+
+/* Output geometry: histogram rows (maxell/2+1), r and k bin counts, and the
+ * r- and k-subgrid shapes (correlator.h:109-205). */
+int fc_corr_dims(const fc_correlator *corr, int *nrows, int *nr, int *nk,
+                 int rshape[3], int kshape[3]);
+
+/* BaseCorrelator::set_grid2 / set_grid2_fft (correlator.h:53-77).  The
+ * complex grid is N0 x N1 x (N2/2+1) interleaved (re, im) doubles. */
+int fc_corr_set_grid2(fc_correlator *corr, const double *host_grid);
+int fc_corr_set_grid2_grid(fc_correlator *corr, const fc_grid *grid2);
+int fc_corr_set_grid2_fft(fc_correlator *corr, const double *host_complex);
+
+/* autocorrelate(grid) and cross_correlate(grid1) against grid2
+ * (correlator.h:262-268, 372-378).  The _grid forms read a device grid. */
+int fc_corr_autocorrelate(fc_correlator *corr, const double *host_grid);
+int fc_corr_autocorrelate_grid(fc_correlator *corr, const fc_grid *grid);
+int fc_corr_cross_correlate(fc_correlator *corr, const double *host_grid1);
+int fc_corr_cross_correlate_grid(fc_correlator *corr, const fc_grid *grid1);
+
+/* Results of the last correlation (correlator.h:80-95).  Any pointer may be
+ * NULL.  Histograms are (nrows, nbins) row-major; counts are int32. */
+int fc_corr_results(const fc_correlator *corr, double *rbins, int *rcounts,
+                    double *rhist, double *kbins, int *kcounts, double *khist,
+                    double *zerolag);
+
+typedef struct fc_corr_timings {
+  double total_time;     /* seconds of device time per phase, last run */
+  double fft_time;
+  double ylm_time;
+  double multiply_time;
+  double extract_time;
+  double histogram_time;
+  double setup_time;
+  int n_fft;             /* cuFFT executions in the last run */
+} fc_corr_timings;
+int fc_corr_timings_get(const fc_correlator *corr, fc_corr_timings *t);
+
+/* Bytes of device memory a correlator of this configuration holds (grids,
+ * subgrids, FFT plans); used for admission by HBM footprint. */
+int fc_corr_footprint(int kind, const int shape[3], double cell_size,
+                      double rmax, double kmax, int maxell, int precision,
+                      size_t *bytes);
+
+/* ---------------------------------------------- asynchronous submission */
+/* Binds the correlator's work to an existing CUDA stream (a cudaStream_t
+ * passed as void*); NULL restores the correlator's own stream. */
+int fc_corr_set_stream(fc_correlator *corr, void *cuda_stream);
+/* Enqueue a correlation of a device grid without waiting for it; results
+ * are valid after fc_corr_synchronize. */
+int fc_corr_autocorrelate_grid_async(fc_correlator *corr, const fc_grid *grid);
+int fc_corr_synchronize(fc_correlator *corr);
+
+/* Per-kernel device time of the correlator's launches, for roofline
+ * accounting.  Off by default; when on, every launch of the correlator is
+ * bracketed by CUDA events on its stream. */
+typedef struct fc_kernel_time {
+  char name[32];   /* kernel family: weight, r2c, c2r, conj_mul, ksub, ... */
+  int launches;    /* launches since profiling was (re)enabled */
+  double seconds;  /* summed device time of those launches */
+} fc_kernel_time;
+int fc_corr_set_profiling(fc_correlator *corr, int enable);
+/* Copies up to max entries; *n receives the number of kernel families. */
+int fc_corr_profile(fc_correlator *corr, fc_kernel_time *out, int max, int *n);
+
+/* --------------------------------------------------------- HistogramList */
+typedef struct fc_hist fc_hist;
+
+/* HistogramList(n, minval, maxval, binsize) (histogram_list.h:12-26). */
+int fc_hist_create(int n, double minval, double maxval, double binsize,
+                   fc_hist **out);
+int fc_hist_destroy(fc_hist *h);
+int fc_hist_nbins(const fc_hist *h, int *nbins);
+/* accumulate(ih, x, y) over len host values (histogram_list.h:33-45):
+ * counts are exact, sums are FP64 in a fixed order. */
+int fc_hist_accumulate(fc_hist *h, int ih, const double *x, const double *y,
+                       int64_t len);
+int fc_hist_reset(fc_hist *h);
+/* Copies bins (nbins), counts and hist_values ((n, nbins)). */
+int fc_hist_get(const fc_hist *h, double *bins, int *counts, double *hist);
+
+/* ------------------------------------------------------------- utilities */
+/* Waits for all work on the current device. */
+int fc_device_synchronize(void);
+/* Page-locks an existing host range so copies from it run at full PCIe
+ * speed (cudaHostRegister), and releases it. */
+int fc_host_register(void *ptr, size_t bytes);
+int fc_host_unregister(void *ptr);
+/* Plain device allocations for callers that stage inputs themselves. */
+int fc_device_malloc(size_t bytes, void **ptr);
+int fc_device_free(void *ptr);
+int fc_memcpy_htod(void *dst, const void *src, size_t bytes);
+/* Device-timeline stopwatch: start and stop synchronise the device and
+ * record an event on the default stream, so the interval covers all work
+ * issued in between on any stream. */
+typedef struct fc_timer fc_timer;
+int fc_timer_create(fc_timer **t);
+int fc_timer_start(fc_timer *t);
+int fc_timer_stop(fc_timer *t, double *seconds);
+int fc_timer_destroy(fc_timer *t);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FC_API_H */

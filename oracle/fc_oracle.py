@@ -362,7 +362,7 @@ def _rfftn(x):
 
 def _irfftn(c, shape):
     # FFTW's c2r is unnormalised: norm="forward" leaves the inverse unscaled.
-    return np.fft.irfftn(c, s=shape, norm="forward")
+    return np.fft.irfftn(c, s=shape, axes=(0, 1, 2), norm="forward")
 
 
 def _result(geo, zerolag):

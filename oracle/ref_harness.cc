@@ -109,7 +109,8 @@ int fcref_grid_coords(const int *shape, const double *posmin, double cell,
 }
 
 // MassAssignor over an (n, 4) posw array, then flush().  stats receives
-// num_added, num_skipped, totw, totwsq (mass_assignor.h:52-58).
+// num_added, num_skipped, totw, totwsq, sort_time, window_time
+// (mass_assignor.h:52-58): six doubles.
 int fcref_mass_assign(const double *posw, long n, const int *shape,
                       const double *posmin, double cell, int scheme,
                       int periodic, long buffer_size, double *grid_out,
@@ -129,6 +130,8 @@ int fcref_mass_assign(const double *posw, long n, const int *shape,
     stats[1] = (double)ma.num_skipped();
     stats[2] = ma.totw();
     stats[3] = ma.totwsq();
+    stats[4] = ma.sort_time();
+    stats[5] = ma.window_time();
   });
 }
 
@@ -136,13 +139,15 @@ int fcref_mass_assign(const double *posw, long n, const int *shape,
 // grid2 == NULL runs autocorrelate(grid1), otherwise
 // cross_correlate(grid1, grid2).  Output arrays are sized by the caller:
 // nrows = maxell/2 + 1, nr = floor(rmax/dr), nk = floor(kmax/dk)
-// (histogram_list.h:15).
+// (histogram_list.h:15).  timers (8 doubles, may be NULL) receives the
+// reference's own phase timers (correlator.h:97-105): setup, fft_plan, fft,
+// extract, multiply, ylm, histogram, total, in seconds.
 int fcref_correlate(int survey, const double *grid1, const double *grid2,
                     const int *shape, double cell, const double *posmin,
                     int window, double rmax, double dr, double kmax, double dk,
                     int maxell, double *rbins, int *rcounts, double *rhist,
                     double *kbins, int *kcounts, double *khist,
-                    double *zerolag, int quiet) {
+                    double *zerolag, int quiet, double *timers) {
   QuietScope q(quiet);
   return guarded([&] {
     std::array<int, 3> shp = {shape[0], shape[1], shape[2]};
@@ -176,6 +181,16 @@ int fcref_correlate(int survey, const double *grid1, const double *grid2,
     std::memcpy(kcounts, kc.data(), sizeof(int) * kc.size());
     std::memcpy(khist, kh.data(), sizeof(double) * kh.size());
     *zerolag = corr->zerolag();
+    if (timers) {
+      timers[0] = corr->setup_time();
+      timers[1] = corr->fft_plan_time();
+      timers[2] = corr->fft_time();
+      timers[3] = corr->extract_time();
+      timers[4] = corr->multiply_time();
+      timers[5] = corr->ylm_time();
+      timers[6] = corr->histogram_time();
+      timers[7] = corr->total_time();
+    }
   });
 }
 
