@@ -430,7 +430,9 @@ struct Assignor {
   DeviceBuffer totals;                 // [totw, totwsq]
   DeviceBuffer counts;                 // [num_added]
   DeviceBuffer staging;                // pos / weights for the (pos, w) forms
-  uint64_t num_skipped_host = 0;       // derived from counts at stats time
+  // Particles being keyed and scattered: the internal buffer, or a caller's
+  // device array that is assigned in place without a copy.
+  const double *src_posw = nullptr;
   uint64_t num_seen = 0;               // particles passed to add calls
   PhaseTimer sort_timer, window_timer;
   double sort_seconds = 0.0, window_seconds = 0.0;
@@ -510,6 +512,23 @@ struct Assignor {
 
   size_t key_bytes() const { return wide_keys ? 8 : 4; }
 
+  // Key/index buffers for assigning `need` particles straight from a
+  // caller's device array (nothing is buffered).
+  void reserve_keys(int64_t need) {
+    FC_REQUIRE(count == 0, FC_ERR_STATE, "particles are still buffered");
+    FC_REQUIRE(need < (int64_t)0xffffffffll, FC_ERR_INVALID,
+               "too many particles in one call (limit 2^32-1)");
+    if ((size_t)need * key_bytes() <= keys.bytes()) return;
+    keys.release();
+    vals.release();
+    keys_alt.release();
+    vals_alt.release();
+    keys.resize(need * key_bytes());
+    vals.resize(need * sizeof(uint32_t));
+    keys_alt.resize(need * key_bytes());
+    vals_alt.resize(need * sizeof(uint32_t));
+  }
+
   // Grows the particle buffer to hold `need` particles, keeping the
   // buffered ones.
   void reserve(int64_t need) {
@@ -543,16 +562,17 @@ struct Assignor {
   // K-key over the particles just placed at [count, count+n).
   void key_new(int64_t n) {
     if (n == 0) return;
+    src_posw = posw.as<double>();
     const unsigned blocks = std::min<unsigned>(kSumBlocks, grid_for(n, 256));
     double *parts = partials.as<double>();
     if (wide_keys) {
       k_keys<uint64_t><<<blocks, 256, 0, stream()>>>(
-          posw.as<double>(), count, n, geom, (uint64_t)ntiles * kTileCells,
+          src_posw, count, n, geom, (uint64_t)ntiles * kTileCells,
           keys.as<uint64_t>(), vals.as<uint32_t>(), parts,
           counts.as<unsigned long long>());
     } else {
       k_keys<uint32_t><<<blocks, 256, 0, stream()>>>(
-          posw.as<double>(), count, n, geom, (uint32_t)(ntiles * kTileCells),
+          src_posw, count, n, geom, (uint32_t)(ntiles * kTileCells),
           keys.as<uint32_t>(), vals.as<uint32_t>(), parts,
           counts.as<unsigned long long>());
     }
@@ -565,6 +585,17 @@ struct Assignor {
 
   void add_device_posw(const double *src, int64_t n, cudaMemcpyKind kind) {
     FC_REQUIRE(n >= 0, FC_ERR_INVALID, "negative particle count");
+    if (kind == cudaMemcpyDeviceToDevice && count == 0 && n > 0 &&
+        n < (int64_t)0xffffffffll && (buffer_size == 0 || n >= buffer_size)) {
+      // Assigned at once: key, sort and scatter straight from the caller's
+      // array instead of copying it into the buffer first.
+      reserve_keys(n);
+      const double *keep = src_posw;
+      key_device(src, n);
+      flush();
+      src_posw = keep;
+      return;
+    }
     int64_t done = 0;
     // Large inputs are assigned in pieces so the buffer stays bounded.
     const int64_t piece_max = (int64_t)1 << 28;
@@ -577,6 +608,27 @@ struct Assignor {
       done += piece;
       maybe_flush();
     }
+  }
+
+  // K-key over an external device array of n particles (buffer empty).
+  void key_device(const double *src, int64_t n) {
+    src_posw = src;
+    const unsigned blocks = std::min<unsigned>(kSumBlocks, grid_for(n, 256));
+    double *parts = partials.as<double>();
+    if (wide_keys) {
+      k_keys<uint64_t><<<blocks, 256, 0, stream()>>>(
+          src, 0, n, geom, (uint64_t)ntiles * kTileCells, keys.as<uint64_t>(),
+          vals.as<uint32_t>(), parts, counts.as<unsigned long long>());
+    } else {
+      k_keys<uint32_t><<<blocks, 256, 0, stream()>>>(
+          src, 0, n, geom, (uint32_t)(ntiles * kTileCells), keys.as<uint32_t>(),
+          vals.as<uint32_t>(), parts, counts.as<unsigned long long>());
+    }
+    FC_LAUNCH_CHECK();
+    k_fold_totals<<<1, 256, 0, stream()>>>(parts, blocks, totals.as<double>());
+    FC_LAUNCH_CHECK();
+    count = n;
+    num_seen += n;
   }
 
   void add_pos(const double *pos, const double *w, double wconst, int64_t n) {
@@ -640,25 +692,25 @@ struct Assignor {
       switch (scheme) {
         case 0:
           k_scatter<0, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<0>(),
-                               stream()>>>(posw.as<double>(), sk, sv,
+                               stream()>>>(src_posw, sk, sv,
                                            tile_start.as<uint32_t>(), ct, geom,
                                            grid->ptr());
           break;
         case 1:
           k_scatter<1, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<1>(),
-                               stream()>>>(posw.as<double>(), sk, sv,
+                               stream()>>>(src_posw, sk, sv,
                                            tile_start.as<uint32_t>(), ct, geom,
                                            grid->ptr());
           break;
         case 2:
           k_scatter<2, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<2>(),
-                               stream()>>>(posw.as<double>(), sk, sv,
+                               stream()>>>(src_posw, sk, sv,
                                            tile_start.as<uint32_t>(), ct, geom,
                                            grid->ptr());
           break;
         default:
           k_scatter<3, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<3>(),
-                               stream()>>>(posw.as<double>(), sk, sv,
+                               stream()>>>(src_posw, sk, sv,
                                            tile_start.as<uint32_t>(), ct, geom,
                                            grid->ptr());
           break;
