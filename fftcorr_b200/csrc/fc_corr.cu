@@ -29,7 +29,11 @@
 #include <type_traits>
 #include <vector>
 
+#include <cstdlib>
+#include <memory>
+
 #include "fc_common.cuh"
+#include "fc_fused.h"
 #include "fc_hist.cuh"
 #include "fc_internal.h"
 
@@ -392,6 +396,8 @@ struct Correlator {
   double shift_value = 0.0;  // mean removed before FP32 transforms
 
   Profiler prof;
+  // Hand-written fused FFT passes for the survey loop (null: cuFFT path).
+  std::unique_ptr<FusedSurvey> fused;
   cufftHandle plan_r2c = 0, plan_c2r = 0;
   DeviceBuffer fft_area;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
@@ -425,8 +431,13 @@ struct Correlator {
     stream = own_stream;
     FC_CUDA(cudaEventCreate(&ev_start));
     FC_CUDA(cudaEventCreate(&ev_stop));
+    const char *mode = std::getenv("FFTCORR_B200_FFT");
+    const bool want_fused = !(mode && std::string(mode) == "cufft");
+    if (kind == FC_SURVEY && want_fused &&
+        FusedSurvey::supported(geo.shape, geo.rsize))
+      fused.reset(new FusedSurvey(geo.shape, geo.rsize, geo.kshape, fp64()));
     allocate();
-    make_plans();
+    if (!fused) make_plans();
     build_bins();
   }
 
@@ -443,7 +454,7 @@ struct Correlator {
   size_t real_bytes() const { return fp64() ? 8 : 4; }
 
   void allocate() {
-    work.resize(geo.nreal_padded() * real_bytes());
+    if (!fused) work.resize(geo.nreal_padded() * real_bytes());
     rsub.resize(geo.rcells() * sizeof(double));
     ksub.resize(geo.kcells() * sizeof(double));
     d_raxis.resize(geo.rsize * sizeof(double));
@@ -524,9 +535,26 @@ struct Correlator {
 
   void set_stream(cudaStream_t s) {
     stream = s ? s : own_stream;
-    FC_CUFFT(cufftSetStream(plan_r2c, stream));
-    FC_CUFFT(cufftSetStream(plan_c2r, stream));
+    if (plan_r2c) FC_CUFFT(cufftSetStream(plan_r2c, stream));
+    if (plan_c2r) FC_CUFFT(cufftSetStream(plan_c2r, stream));
   }
+
+  KAxes kaxes() const {
+    const double *ax = d_kaxes.as<double>();
+    const double *wn = d_kwin.as<double>();
+    const int a = geo.kshape[0], b = geo.kshape[1];
+    return KAxes{ax, ax + a, ax + a + b, wn, wn + a, wn + a + b};
+  }
+
+  // Adapter from the fused passes' hooks to the profiler.
+  struct ProfHook : PhaseHook {
+    Profiler *p;
+    cudaStream_t s;
+    std::unique_ptr<Profiler::Scope> cur;
+    ProfHook(Profiler *p_, cudaStream_t s_) : p(p_), s(s_) {}
+    void begin(const char *name) override { cur.reset(new Profiler::Scope(p, s, name)); }
+    void end() override { cur.reset(); }
+  };
 
   // ------------------------------------------------------------ kernels
 
@@ -638,6 +666,14 @@ struct Correlator {
   template <typename T>
   void set_grid2_dev(const double *rho) {
     using C = typename Cplx<T>::type;
+    if (fused) {
+      ProfHook hook(&prof, stream);
+      hook.begin("grid2");
+      fused->grid2(fused->prepare_input(rho, stream), stream, kaxes());
+      hook.end();
+      have_g2 = true;
+      return;
+    }
     g2.resize(geo.ncomplex() * sizeof(C));
     copy_pad<T>(rho, shift_for(rho));
     exec_r2c(work.get(), g2.get());
@@ -652,6 +688,23 @@ struct Correlator {
 
   void set_grid2_fft_host(const double *host_complex) {
     const size_t nc = geo.ncomplex();
+    if (fused) {
+      if (fp64()) {
+        FC_CUDA(cudaMemcpyAsync(fused->g_data(), host_complex,
+                                nc * sizeof(double2), cudaMemcpyHostToDevice,
+                                stream));
+      } else {
+        DeviceBuffer tmp(nc * sizeof(double2));
+        FC_CUDA(cudaMemcpyAsync(tmp.get(), host_complex, nc * sizeof(double2),
+                                cudaMemcpyHostToDevice, stream));
+        k_z2c<<<grid_for(nc, 256), 256, 0, stream>>>(
+            tmp.as<double2>(), static_cast<float2 *>(fused->g_data()), nc);
+        FC_LAUNCH_CHECK();
+        FC_CUDA(cudaStreamSynchronize(stream));
+      }
+      have_g2 = true;
+      return;
+    }
     if (fp64()) {
       g2.resize(nc * sizeof(double2));
       FC_CUDA(cudaMemcpyAsync(g2.get(), host_complex, nc * sizeof(double2),
@@ -704,6 +757,21 @@ struct Correlator {
   void survey_run(const double *rho) {
     const size_t ncells = geo.ncells();
     const int maxell = 2 * (geo.nrows - 1);
+    if (fused) {
+      const void *in = fused->prepare_input(rho, stream);
+      ProfHook hook(&prof, stream);
+      const KAxes ka = kaxes();
+      for (int ell = 0; ell <= maxell; ell += 2) {
+        zero_sub(true, true);
+        for (int m = -ell; m <= ell; ++m)
+          fused->term(in, ell, m, xyz0, (double)ncells, ksub.as<double>(),
+                      rsub.as<double>(), d_raxis.as<double>(), ka, stream,
+                      prof.on ? &hook : nullptr);
+        hist_rows(ell, true, true);
+        if (ell == 0) save_zerolag();
+      }
+      return;
+    }
     for (int ell = 0; ell <= maxell; ell += 2) {
       zero_sub(true, true);
       for (int m = -ell; m <= ell; ++m) {

@@ -1,0 +1,272 @@
+// fc_fft.cuh -- shared-memory Stockham FFT engine for the fused correlator
+// passes.
+//
+// A CTA transforms B columns of length L held in shared memory as
+// buf[i * BP + b] (row i of column b, BP = B + 1 to spread banks).  The
+// transform is an iterative mixed-radix Stockham autosort (radices 8, 4, 2,
+// 3, 5, 7) between two shared buffers: each pass reads a butterfly's R
+// inputs, applies the twiddles and the radix-R DFT in registers and writes
+// the outputs to their Stockham positions in the other buffer.  Twiddles come from a table of e^{-2 pi i m / Lt} (Lt a
+// multiple of L) computed in FP64 on the host.  Forward is sign -1 and the
+// inverse is unnormalised, as in FFTW and cuFFT.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fc {
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) {
+  C r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) {
+  C r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+// a * conj(b)
+template <typename C>
+__device__ __forceinline__ C cmulc(C a, C b) {
+  C r;
+  r.x = a.x * b.x + a.y * b.y;
+  r.y = a.y * b.x - a.x * b.y;
+  return r;
+}
+template <typename C>
+__device__ __forceinline__ C cconj(C a) {
+  C r;
+  r.x = a.x;
+  r.y = -a.y;
+  return r;
+}
+// (sign * i) * a
+template <typename C>
+__device__ __forceinline__ C cmuli(C a, int sign) {
+  C r;
+  r.x = -sign * a.y;
+  r.y = sign * a.x;
+  return r;
+}
+template <typename C, typename T>
+__device__ __forceinline__ C cscale(C a, T s) {
+  C r;
+  r.x = a.x * s;
+  r.y = a.y * s;
+  return r;
+}
+
+// Radix-R DFT in registers: out[q] = sum_u v[u] * e^{sign 2 pi i u q / R}.
+template <int R, typename C>
+struct Dft;
+
+template <typename C>
+struct Dft<2, C> {
+  __device__ static void run(C *v, int) {
+    const C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <typename C>
+struct Dft<4, C> {
+  __device__ static void run(C *v, int sign) {
+    const C a0 = cadd(v[0], v[2]);
+    const C a1 = csub(v[0], v[2]);
+    const C a2 = cadd(v[1], v[3]);
+    const C d = cmuli(csub(v[1], v[3]), sign);
+    v[0] = cadd(a0, a2);
+    v[2] = csub(a0, a2);
+    v[1] = cadd(a1, d);
+    v[3] = csub(a1, d);
+  }
+};
+
+template <typename C>
+struct Dft<8, C> {
+  // Radix 2 across stride 4, then two radix-4 DFTs (even and odd outputs).
+  __device__ static void run(C *v, int sign) {
+    using T = decltype(v[0].x);
+    const T h = (T)0.70710678118654752440;
+    C a[4], b[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a[u] = cadd(v[u], v[u + 4]);
+      b[u] = csub(v[u], v[u + 4]);
+    }
+    // b[u] *= e^{sign 2 pi i u / 8}
+    {
+      C t = b[1];
+      b[1].x = h * (t.x - sign * t.y);
+      b[1].y = h * (t.y + sign * t.x);
+      b[2] = cmuli(b[2], sign);
+      t = b[3];
+      b[3].x = h * (-t.x - sign * t.y);
+      b[3].y = h * (-t.y + sign * t.x);
+    }
+    Dft<4, C>::run(a, sign);
+    Dft<4, C>::run(b, sign);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      v[2 * p] = a[p];
+      v[2 * p + 1] = b[p];
+    }
+  }
+};
+
+template <typename C>
+struct Dft<3, C> {
+  __device__ static void run(C *v, int sign) {
+    using T = decltype(v[0].x);
+    const T s3 = (T)0.86602540378443864676 * sign;
+    const C t = cadd(v[1], v[2]);
+    const C d = csub(v[1], v[2]);
+    C m;
+    m.x = v[0].x - (T)0.5 * t.x;
+    m.y = v[0].y - (T)0.5 * t.y;
+    C sd;
+    sd.x = -s3 * d.y;
+    sd.y = s3 * d.x;
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(m, sd);
+    v[2] = csub(m, sd);
+  }
+};
+
+// Generic odd prime radix (5, 7): O(R^2) complex products with the R-th
+// roots of unity evaluated once per butterfly by sincospi (correctly
+// rounded to within an ulp); these radices are rare in practice.
+template <int R, typename C>
+struct DftGeneric {
+  __device__ static void run(C *v, int sign) {
+    using T = decltype(v[0].x);
+    C w[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      double s, c;
+      sincospi(2.0 * m / R, &s, &c);
+      w[m].x = (T)c;
+      w[m].y = (T)(sign * s);
+    }
+    C in[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) in[u] = v[u];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      C acc = in[0];
+#pragma unroll
+      for (int u = 1; u < R; ++u) acc = cadd(acc, cmul(in[u], w[(u * q) % R]));
+      v[q] = acc;
+    }
+  }
+};
+template <typename C>
+struct Dft<5, C> : DftGeneric<5, C> {};
+template <typename C>
+struct Dft<7, C> : DftGeneric<7, C> {};
+
+// Plan of one transform length: up to 12 passes.
+struct FftPlan {
+  int L;          // transform length
+  int npass;
+  int radix[12];
+  int ns[12];     // product of the radices before each pass
+  int tab_scale;  // root-table order / L
+};
+
+// One Stockham pass of radix R: reads the B columns from src, writes the
+// result to dst (both [L][BP] in shared memory).  Each thread handles one
+// butterfly at a time, so only R complex values live in registers.
+template <int R, typename C>
+__device__ __forceinline__ void stockham_pass(const C *src, C *dst, int L,
+                                              int B, int BP, int Ns,
+                                              const C *__restrict__ tab,
+                                              int tab_scale, int sign) {
+  const int LR = L / R;
+  const int nbf = LR * B;
+  const int step = (L / (Ns * R)) * tab_scale;
+  const int Lt = L * tab_scale;
+  for (int bf = threadIdx.x; bf < nbf; bf += blockDim.x) {
+    const int j = bf / B;
+    const int b = bf - j * B;
+    const int k = j % Ns;
+    C v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = src[(j + q * LR) * BP + b];
+    if (Ns > 1) {
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        C w = tab[(q * k * step) % Lt];
+        if (sign > 0) w.y = -w.y;
+        v[q] = cmul(v[q], w);
+      }
+    }
+    Dft<R, C>::run(v, sign);
+    const int o = ((j - k) * R + k) * BP + b;
+#pragma unroll
+    for (int q = 0; q < R; ++q) dst[o + q * Ns * BP] = v[q];
+  }
+  __syncthreads();
+}
+
+// Transforms the B columns in a (the caller has synchronised after filling
+// it), ping-ponging with b; returns the buffer that holds the result
+// (synchronised).
+template <typename C>
+__device__ C *fft_columns(C *a, C *b, const FftPlan &p, int B, int BP,
+                          const C *__restrict__ tab, int sign) {
+  C *src = a, *dst = b;
+  for (int s = 0; s < p.npass; ++s) {
+    const int R = p.radix[s];
+    const int Ns = p.ns[s];
+    switch (R) {
+      case 8:
+        stockham_pass<8>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        break;
+      case 4:
+        stockham_pass<4>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        break;
+      case 2:
+        stockham_pass<2>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        break;
+      case 3:
+        stockham_pass<3>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        break;
+      case 5:
+        stockham_pass<5>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        break;
+      default:
+        stockham_pass<7>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        break;
+    }
+    C *t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+}  // namespace fc

@@ -1,0 +1,84 @@
+// fc_fused.h -- fused hand-written FFT passes of the survey correlator
+// (see fc_fused.cu for the algorithm).
+#pragma once
+
+#include <vector>
+
+#include "fc_common.cuh"
+#include "fc_fft.cuh"
+
+namespace fc {
+
+// Geometry shared by the fused kernels (passed by value).
+struct FusedGeom {
+  int n0, n1, n2;  // grid shape
+  int m;           // N2 / 2: complex length of the z transform
+  int h;           // N2 / 2 + 1: half-complex z extent
+  int rs, ro;      // r-subgrid edge and its centre offset (rs / 2)
+  int ks0, ks1, ks2;  // k-subgrid shape
+  FftPlan px, py, pz;
+};
+
+// Device pointers of the k axes and the per-axis |W|^2 window tables.
+struct KAxes {
+  const double *kx, *ky, *kz, *wx, *wy, *wz;
+};
+
+// Optional per-pass timing callbacks (the correlator's profiler).
+struct PhaseHook {
+  virtual void begin(const char *name) = 0;
+  virtual void end() = 0;
+  virtual ~PhaseHook() {}
+};
+
+class FusedSurvey {
+ public:
+  // True when every transform length factors into 2, 3, 5, 7, N2 is even
+  // and the shared-memory tiles fit.
+  static bool supported(const int shape[3], int rsize);
+
+  FusedSurvey(const int shape[3], int rsize, const int kshape[3], bool fp64);
+
+  // The grid in the arithmetic of the passes: rho itself in FP64, an FP32
+  // copy in mixed precision.
+  const void *prepare_input(const double *rho, cudaStream_t s);
+  // G = 3-D DFT of the prepared grid (BaseCorrelator::set_grid2).
+  void grid2(const void *rho_in, cudaStream_t s, const KAxes &ka);
+  // One (ell, m) term of Correlator::correlate_internal, accumulated into
+  // the FP64 subgrids.
+  void term(const void *rho_in, int ell, int m, const double xyz0[3],
+            double ncells, double *ksub, double *rsub, const double *raxis,
+            const KAxes &ka, cudaStream_t s, PhaseHook *hook);
+
+  // G in the half-complex layout [N0][N1][N2/2+1] (FP64 or FP32 complex).
+  void *g_data() const { return G.get(); }
+  bool fp64() const { return fp64_; }
+
+  FusedGeom g;
+
+ private:
+  template <typename V>
+  void upload(DeviceBuffer &dst, const std::vector<V> &v);
+  size_t smem(int L, int B) const;
+  void set_smem_limits();
+  template <typename T>
+  void zfwd(const void *rho, bool weight, const YlmParams &p,
+            const double xyz0[3], cudaStream_t s);
+  template <typename T>
+  void yfwd(cudaStream_t s);
+  template <typename T>
+  void xcorr(bool product, double *ksub, const KAxes &ka, const YlmParams &pk,
+             cudaStream_t s);
+  template <typename T>
+  void yinv(cudaStream_t s);
+  template <typename T>
+  void zinv(double *rsub, const double *raxis, const YlmParams &pr,
+            cudaStream_t s);
+
+  bool fp64_;
+  int bx = 1, by = 1, bz = 1;  // columns per CTA of each axis
+  DeviceBuffer tabx, taby, tabz;
+  DeviceBuffer W, G, Wr, Wry, rho32;
+};
+
+}  // namespace fc

@@ -205,6 +205,15 @@ def test_grid_host_mirror_semantics():
 
 # ------------------------------------------------------------ correlators
 
+@pytest.fixture(params=["fused", "cufft"])
+def fft_path(request, monkeypatch):
+    """Runs a survey test through the hand-written fused FFT passes and
+    through the cuFFT path (the correlator reads FFTCORR_B200_FFT when it is
+    created)."""
+    monkeypatch.setenv("FFTCORR_B200_FFT", request.param)
+    return request.param
+
+
 def _periodic_field(shape, cell, seed, scheme=3):
     box = np.array(shape) * cell
     posw = clustered_catalog(60000, [0, 0, 0], box, seed, ncenters=40,
@@ -242,7 +251,7 @@ def test_periodic_correlator_fp64(maxell, window):
 
 
 @pytest.mark.parametrize("maxell", [0, 2, 4])
-def test_survey_correlator_fp64(maxell):
+def test_survey_correlator_fp64(maxell, fft_path):
     shape, cell = (32, 36, 40), 12.0
     posmin = np.array([-100.0, 250.0, -300.0])
     nn, _ = _survey_field(shape, cell, posmin, 31)
@@ -255,7 +264,7 @@ def test_survey_correlator_fp64(maxell):
     assert list(ps.colnames) == ["k", "ps", "histogram", "count"]
 
 
-def test_correlators_read_device_grids():
+def test_correlators_read_device_grids(fft_path):
     shape, cell = (32, 32, 32), 15.0
     posmin = np.array([-240.0, -240.0, 10.0])
     nn, _ = _survey_field(shape, cell, posmin, 41)
@@ -268,7 +277,7 @@ def test_correlators_read_device_grids():
     _compare_results(c.results(), ref, FP64_RTOL, "survey-device")
 
 
-def test_cross_correlations():
+def test_cross_correlations(fft_path):
     shape, cell = (24, 24, 32), 10.0
     a = _periodic_field(shape, cell, 51)
     b = _periodic_field(shape, cell, 52, scheme=1)
@@ -291,13 +300,28 @@ def test_cross_correlations():
     _compare_results(s.results(), sref, FP64_RTOL, "survey-cross")
 
 
+@pytest.mark.parametrize("shape", [(20, 28, 30), (24, 18, 50), (16, 16, 33)])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_survey_radix_3_5_7_and_odd_sizes(shape, precision):
+    """Lengths with factors 3, 5, 7 run through the fused passes; an odd N2
+    uses the cuFFT path.  Both must match the oracle."""
+    cell = 10.0
+    posmin = np.array([-100.0, 50.0, -130.0])
+    nn, _ = _survey_field(shape, cell, posmin, 81)
+    args = (cell, posmin, TSC_CORRECTION, 45.0, 6.0, 0.2, 0.03, 4)
+    ref = O.survey_correlate(nn, *args)
+    c = fb.Correlator(shape, *args, precision=precision)
+    c.autocorrelate(nn)
+    _compare_results(c.results(), ref, FP64_RTOL, "radix", fp32=precision == "fp32")
+
+
 def test_cross_correlate_without_grid2_fails():
     c = fb.PeriodicCorrelator((16, 16, 16), 10.0, 0, 30.0, 5.0, 0.2, 0.05, 0)
     with pytest.raises(_lib.FcError):
         c.cross_correlate(np.zeros((16, 16, 16)))
 
 
-def test_fp32_mixed_within_tolerance():
+def test_fp32_mixed_within_tolerance(fft_path):
     shape, cell = (48, 48, 48), 12.0
     posmin = np.array([-288.0, -288.0, 30.0])
     nn, rr = _survey_field(shape, cell, posmin, 61)
@@ -315,7 +339,7 @@ def test_fp32_mixed_within_tolerance():
     _compare_results(c.results(), ref, 0, "periodic-fp32", fp32=True)
 
 
-def test_correlation_is_deterministic():
+def test_correlation_is_deterministic(fft_path):
     shape, cell = (32, 32, 32), 10.0
     posmin = np.array([-160.0, -160.0, 20.0])
     nn, _ = _survey_field(shape, cell, posmin, 71)
@@ -371,7 +395,7 @@ def _gpu_cli(cats, header, ngrid=(256, 256, 256), sep=200.0, dsep=10.0,
 
 
 @pytest.mark.parametrize("hemi", ["north", "south"])
-def test_golden_tables_through_gpu(hemi, golden_catalogs, golden_tables):
+def test_golden_tables_through_gpu(hemi, golden_catalogs, golden_tables, fft_path):
     header = golden_catalogs[f"{hemi}_header"]
     DD = golden_catalogs[f"{hemi}_DD"]
     RR = golden_catalogs[f"{hemi}_RR"]
