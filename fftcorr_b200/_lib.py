@@ -122,6 +122,8 @@ _SIGNATURES = {
     "fc_corr_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "fc_corr_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(KernelTime),
                                        ctypes.c_int, c_int_p]),
+    "fc_sum_sumsq_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_double_p,
+                                           c_double_p]),
     "fc_device_synchronize": (ctypes.c_int, []),
     "fc_host_register": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t]),
     "fc_host_unregister": (ctypes.c_int, [ctypes.c_void_p]),

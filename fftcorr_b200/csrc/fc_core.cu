@@ -293,6 +293,89 @@ int fc_grid_axpy(fc_grid *y, double a, const fc_grid *x) {
 
 }  // extern "C"
 
+// ============================================= allocation-free reduction
+
+namespace fc {
+namespace {
+
+// Elements per block of the allocation-free reduction: block b sums
+// [b * kStaticSeg, (b + 1) * kStaticSeg) in a fixed order.
+constexpr int64_t kStaticSeg = 1 << 18;
+constexpr int kStaticParts = 4096;  // FC_SUM_STATIC_MAX_N / kStaticSeg
+
+// Scratch of fc_sum_sumsq_static: kStaticParts (sum, sumsq) partials and
+// the two results, 64 KiB + 16 B.  Host code must not use this name as an
+// address; it uses the device address looked up below.
+static __device__ __align__(256) double g_static_scratch[2 * kStaticParts + 2];
+
+__global__ void k_seg_partials(const double *a, int64_t n, double *partials) {
+  __shared__ double red[32];
+  const int64_t lo = (int64_t)blockIdx.x * kStaticSeg;
+  const int64_t hi = lo + kStaticSeg < n ? lo + kStaticSeg : n;
+  double s = 0.0, q = 0.0;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double v = a[i];
+    s += v;
+    q += v * v;
+  }
+  s = block_sum(s, red);
+  q = block_sum(q, red);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = s;
+    partials[2 * blockIdx.x + 1] = q;
+  }
+}
+
+std::mutex g_static_mu;
+double *g_static_addr[64] = {nullptr};
+
+// Device address of g_static_scratch on the current device, looked up once
+// per device with that device current.
+double *static_scratch() {
+  int dev = 0;
+  FC_CUDA(cudaGetDevice(&dev));
+  FC_REQUIRE(dev >= 0 && dev < 64, FC_ERR_UNSUPPORTED, "device index >= 64");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void *p = nullptr;
+    FC_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+    g_static_addr[dev] = static_cast<double *>(p);
+  }
+  return g_static_addr[dev];
+}
+
+}  // namespace
+}  // namespace fc
+
+extern "C" int fc_sum_sumsq_static(const double *device_data, int64_t n,
+                                   double *sum, double *sumsq) {
+  using namespace fc;
+  return guard([&] {
+    FC_REQUIRE(n >= 0, FC_ERR_INVALID, "n must be non-negative");
+    FC_REQUIRE(n <= FC_SUM_STATIC_MAX_N, FC_ERR_RANGE,
+               "n exceeds FC_SUM_STATIC_MAX_N (2^30 values), the capacity of "
+               "the fixed scratch array");
+    FC_REQUIRE(device_data || n == 0, FC_ERR_INVALID, "null device pointer");
+    double *scr = static_scratch();
+    const int blocks = (int)((n + kStaticSeg - 1) / kStaticSeg);
+    cudaStream_t s = 0;
+    if (blocks > 0) {
+      k_seg_partials<<<blocks, 256, 0, s>>>(device_data, n, scr);
+      FC_LAUNCH_CHECK();
+      k_sum_final<<<1, 256, 0, s>>>(scr, blocks, scr + 2 * kStaticParts);
+      FC_LAUNCH_CHECK();
+    } else {
+      FC_CUDA(cudaMemsetAsync(scr + 2 * kStaticParts, 0, 2 * sizeof(double), s));
+    }
+    double res[2];
+    FC_CUDA(cudaMemcpyAsync(res, scr + 2 * kStaticParts, sizeof(res),
+                            cudaMemcpyDeviceToHost, s));
+    FC_CUDA(cudaStreamSynchronize(s));
+    if (sum) *sum = res[0];
+    if (sumsq) *sumsq = res[1];
+  });
+}
+
 // ============================================================ utilities
 
 namespace {

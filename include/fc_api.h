@@ -230,6 +230,23 @@ int fc_hist_reset(fc_hist *h);
 /* Copies bins (nbins), counts and hist_values ((n, nbins)). */
 int fc_hist_get(const fc_hist *h, double *bins, int *counts, double *hist);
 
+/* ----------------------------------------------- allocation-free variant */
+/* Sum and sum of squares of n FP64 values already in device memory, like
+ * fc_grid_sum, for callers that cannot allocate device memory: code that
+ * runs where cudaMalloc is not allowed (it would synchronise the device or
+ * draw on memory the host application reserves for itself).  This entry
+ * point allocates nothing: its scratch is a fixed 64 KiB array in the
+ * library's own device memory, which every GPU that loads the library holds
+ * until the process exits.  n may be at most FC_SUM_STATIC_MAX_N; larger n
+ * is rejected with FC_ERR_RANGE.  The first call on a device looks up the
+ * scratch address, so make that first call before any stream capture.  All
+ * calls share the one scratch array, so calls that overlap on the GPU (from
+ * several host threads) race; this call waits for its result before
+ * returning.  Has no counterpart in the reference. */
+#define FC_SUM_STATIC_MAX_N (1LL << 30)
+int fc_sum_sumsq_static(const double *device_data, int64_t n, double *sum,
+                        double *sumsq);
+
 /* ------------------------------------------------------------- utilities */
 /* Waits for all work on the current device. */
 int fc_device_synchronize(void);
