@@ -26,12 +26,15 @@ SOURCES = ["fc_core.cu", "fc_hist.cu", "fc_assign.cu", "fc_fused.cu", "fc_corr.c
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17",
-    # Products are rounded one by one like the reference's FP64 code.
-    "-fmad=false",
+    "-O3", "-lineinfo", "-std=c++20",
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
     "--expt-relaxed-constexpr",
 ]
+# Products are rounded one by one like the reference's FP64 code, except in
+# the FFT passes, where fused multiply-adds only change rounding inside the
+# transform (which differs from FFTW's anyway) and halve the arithmetic.
+NO_FMAD = ["-fmad=false"]
+FMAD_OK = {"fc_fused.cu"}
 
 
 def _run(cmd, cwd=None):
@@ -77,6 +80,9 @@ def needs_rebuild():
 def build(reference=DEFAULT_REFERENCE, force=False, verbose_ptxas=False):
     generate_d12(reference)
     if not force and not needs_rebuild():
+        if not os.path.exists(CLI) or os.path.getmtime(CLI) < os.path.getmtime(
+                os.path.join(CSRC, "fftcorr_cli.cc")):
+            build_cli()
         return LIB
     if not os.path.exists(NVCC):
         raise RuntimeError(f"nvcc not found at {NVCC}")
@@ -86,7 +92,8 @@ def build(reference=DEFAULT_REFERENCE, force=False, verbose_ptxas=False):
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        _run([NVCC, *NVCC_FLAGS, *extra, "-I", CSRC, "-c",
+        fmad = [] if os.path.basename(src) in FMAD_OK else NO_FMAD
+        _run([NVCC, *NVCC_FLAGS, *fmad, *extra, "-I", CSRC, "-c",
               src, "-o", obj])
         objs.append(obj)
     tmp = LIB + ".tmp"
@@ -94,7 +101,19 @@ def build(reference=DEFAULT_REFERENCE, force=False, verbose_ptxas=False):
           *objs, "-o", tmp, "-L", os.path.join(CUDA_HOME, "lib64"), "-lcufft",
           "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")])
     os.replace(tmp, LIB)
+    build_cli()
     return LIB
+
+
+CLI = os.path.join(HERE, "bin", "fftcorr")
+
+
+def build_cli():
+    """The `fftcorr` command-line driver (csrc/fftcorr_cli.cc) on the library."""
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    _run(["g++", "-O2", "-std=c++17", os.path.join(CSRC, "fftcorr_cli.cc"),
+          "-o", CLI, "-L", HERE, "-lfftcorr_b200", "-Wl,-rpath,$ORIGIN/.."])
+    return CLI
 
 
 def main(argv=None):

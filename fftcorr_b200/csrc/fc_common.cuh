@@ -209,6 +209,8 @@ struct YlmParams {
   int m;
   double isqpi;
   double value0;
+  double norm;  // isqpi times the (ell, m) constant: the FP32 evaluator's
+                // single normalisation factor, formed in FP64
 };
 
 YlmParams make_ylm_params(int ell, int m, double coeff);
@@ -276,6 +278,46 @@ __device__ __forceinline__ double ylm_eval(const YlmParams &p, double D,
       return D * isqpi * 3.0 / 16.0 * sqrt(35.0 / 2.0) *
              (4.0 * x * (x2 * y - y3)) * ir2 * ir2;
   }
+}
+
+// FP32-mixed evaluator: the same real-form Y_lm * coeff * D, with the
+// observer-relative coordinates formed in FP64 by the caller and the FP64
+// normalisation p.norm, but the angular polynomial and 1/r^2 in FP32 (the
+// result feeds an FP32 transform).
+__device__ __forceinline__ float ylm_eval_f32(const YlmParams &p, float D,
+                                              double xd, double yd, double zd) {
+  if (p.ell == 0) return D * (float)p.value0;
+  const float x = (float)xd, y = (float)yd, z = (float)zd;
+  const float x2 = x * x, y2 = y * y, z2 = z * z;
+  const float ir2 = 1.0f / (x2 + y2 + z2 + 1e-20f);
+  const float n = (float)p.norm;
+  float poly;
+  if (p.ell == 2) {
+    switch (p.m) {
+      case 2: poly = x2 - y2; break;
+      case 1: poly = x * z; break;
+      case 0: poly = 2.0f * z2 - x2 - y2; break;
+      case -1: poly = y * z; break;
+      default: poly = x * y; break;
+    }
+    return D * n * poly * ir2;
+  }
+  const float y4 = y2 * y2;
+  switch (p.m) {
+    case 4: poly = x2 * x2 - 6.0f * x2 * y2 + y4; break;
+    case 3: poly = (x2 - 3.0f * y2) * z * x; break;
+    case 2: poly = 6.0f * z2 * (x2 - y2) - x2 * x2 + y4; break;
+    case 1: poly = (4.0f / 3.0f * z2 - x2 - y2) * x * z; break;
+    case 0:
+      poly = z2 * z2 - 3.0f * z2 * (x2 + y2) +
+             0.375f * (x2 * x2 + 2.0f * x2 * y2 + y4);
+      break;
+    case -1: poly = (4.0f / 3.0f * z2 - x2 - y2) * y * z; break;
+    case -2: poly = 2.0f * x * y * (6.0f * z2 - x2 - y2); break;
+    case -3: poly = (3.0f * x2 * y - y2 * y) * z; break;
+    default: poly = 4.0f * x * (x2 * y - y2 * y); break;
+  }
+  return D * n * poly * (ir2 * ir2);
 }
 
 }  // namespace fc

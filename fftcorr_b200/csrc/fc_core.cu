@@ -47,6 +47,21 @@ YlmParams make_ylm_params(int ell, int m, double coeff) {
   isqpi *= coeff;
   if (m != 0) isqpi *= sqrt(2.0);
   p.isqpi = isqpi;
+  // The (ell, m) constant of each real-form Y_lm (spherical_harmonics.h:
+  // 107-176), folded with isqpi for the FP32 evaluator.
+  double c = 1.0;
+  if (ell == 2) {
+    c = m == 2 ? sqrt(15.0 / 32.0) : m == 0 ? sqrt(5.0 / 16.0) : sqrt(15.0 / 8.0);
+  } else if (ell == 4) {
+    switch (m < 0 ? -m : m) {
+      case 4: c = 3.0 / 16.0 * sqrt(35.0 / 2.0); break;
+      case 3: c = 3.0 / 8.0 * sqrt(35.0); break;
+      case 2: c = 3.0 / 8.0 * sqrt(5.0 / 2.0); break;
+      case 1: c = 3.0 / 8.0 * sqrt(5.0) * 3.0; break;
+      default: c = 3.0 / 16.0 * 8.0; break;
+    }
+  }
+  p.norm = isqpi * c;
   return p;
 }
 

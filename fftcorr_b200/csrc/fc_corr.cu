@@ -671,6 +671,7 @@ struct Correlator {
       hook.begin("grid2");
       fused->grid2(fused->prepare_input(rho, stream), stream, kaxes());
       hook.end();
+      ++n_fft;
       have_g2 = true;
       return;
     }
@@ -763,10 +764,12 @@ struct Correlator {
       const KAxes ka = kaxes();
       for (int ell = 0; ell <= maxell; ell += 2) {
         zero_sub(true, true);
-        for (int m = -ell; m <= ell; ++m)
+        for (int m = -ell; m <= ell; ++m) {
           fused->term(in, ell, m, xyz0, (double)ncells, ksub.as<double>(),
                       rsub.as<double>(), d_raxis.as<double>(), ka, stream,
                       prof.on ? &hook : nullptr);
+          n_fft += 2;  // one forward and one (pruned) inverse transform
+        }
         hist_rows(ell, true, true);
         if (ell == 0) save_zerolag();
       }

@@ -194,32 +194,36 @@ struct FftPlan {
   int npass;
   int radix[12];
   int ns[12];     // product of the radices before each pass
+  int nsmask[12]; // ns - 1 when ns is a power of two, else -1
   int tab_scale;  // root-table order / L
 };
 
 // One Stockham pass of radix R: reads the B columns from src, writes the
 // result to dst (both [L][BP] in shared memory).  Each thread handles one
-// butterfly at a time, so only R complex values live in registers.
-template <int R, typename C>
+// butterfly at a time, so only R complex values live in registers.  B is a
+// compile-time constant so the butterfly decomposition is shifts and masks.
+template <int R, int B, typename C>
 __device__ __forceinline__ void stockham_pass(const C *src, C *dst, int L,
-                                              int B, int BP, int Ns,
+                                              int Ns, int nsmask,
                                               const C *__restrict__ tab,
                                               int tab_scale, int sign) {
+  constexpr int BP = B + 1;
   const int LR = L / R;
   const int nbf = LR * B;
   const int step = (L / (Ns * R)) * tab_scale;
-  const int Lt = L * tab_scale;
   for (int bf = threadIdx.x; bf < nbf; bf += blockDim.x) {
     const int j = bf / B;
     const int b = bf - j * B;
-    const int k = j % Ns;
+    const int k = nsmask >= 0 ? (j & nsmask) : (j % Ns);
     C v[R];
 #pragma unroll
     for (int q = 0; q < R; ++q) v[q] = src[(j + q * LR) * BP + b];
     if (Ns > 1) {
+      // q * k * step < L * tab_scale: no reduction needed.
+      const int ks = k * step;
 #pragma unroll
       for (int q = 1; q < R; ++q) {
-        C w = tab[(q * k * step) % Lt];
+        C w = __ldg(&tab[q * ks]);
         if (sign > 0) w.y = -w.y;
         v[q] = cmul(v[q], w);
       }
@@ -235,31 +239,32 @@ __device__ __forceinline__ void stockham_pass(const C *src, C *dst, int L,
 // Transforms the B columns in a (the caller has synchronised after filling
 // it), ping-ponging with b; returns the buffer that holds the result
 // (synchronised).
-template <typename C>
-__device__ C *fft_columns(C *a, C *b, const FftPlan &p, int B, int BP,
+template <int B, typename C>
+__device__ C *fft_columns(C *a, C *b, const FftPlan &p,
                           const C *__restrict__ tab, int sign) {
   C *src = a, *dst = b;
   for (int s = 0; s < p.npass; ++s) {
     const int R = p.radix[s];
     const int Ns = p.ns[s];
+    const int m = p.nsmask[s];
     switch (R) {
       case 8:
-        stockham_pass<8>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        stockham_pass<8, B>(src, dst, p.L, Ns, m, tab, p.tab_scale, sign);
         break;
       case 4:
-        stockham_pass<4>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        stockham_pass<4, B>(src, dst, p.L, Ns, m, tab, p.tab_scale, sign);
         break;
       case 2:
-        stockham_pass<2>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        stockham_pass<2, B>(src, dst, p.L, Ns, m, tab, p.tab_scale, sign);
         break;
       case 3:
-        stockham_pass<3>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        stockham_pass<3, B>(src, dst, p.L, Ns, m, tab, p.tab_scale, sign);
         break;
       case 5:
-        stockham_pass<5>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        stockham_pass<5, B>(src, dst, p.L, Ns, m, tab, p.tab_scale, sign);
         break;
       default:
-        stockham_pass<7>(src, dst, p.L, B, BP, Ns, tab, p.tab_scale, sign);
+        stockham_pass<7, B>(src, dst, p.L, Ns, m, tab, p.tab_scale, sign);
         break;
     }
     C *t = src;
@@ -267,6 +272,123 @@ __device__ C *fft_columns(C *a, C *b, const FftPlan &p, int B, int BP,
     dst = t;
   }
   return src;
+}
+
+}  // namespace fc
+
+namespace fc {
+
+// ---------------------------------------------------------------------------
+// Register-resident FFT for power-of-two lengths 64 <= L <= 4096.
+//
+// A column of length L is owned by TPC = L/8 threads; thread t holds the
+// eight elements v[u] = x[t + TPC*u].  That is exactly the input of the
+// Stockham radix-8 butterfly j = t, so every pass is a DFT8 in registers and
+// the passes exchange data through shared memory (write, barrier, read,
+// barrier).  A radix-2 or radix-4 pass comes first when L is not a power of
+// 8.  After the last radix-8 pass (Ns = L/8, k = t) thread t holds the
+// natural-order outputs x[t + TPC*q], so the result is stored straight from
+// registers.  Twiddles of a pass are w^q, w = e^{sign 2 pi i k/(8 Ns)}: w,
+// w^2 and w^4 come from the order-L root table and the rest are products.
+// ---------------------------------------------------------------------------
+
+template <typename C>
+__device__ __forceinline__ C tw_load(const C *__restrict__ tab, int idx,
+                                     int sign) {
+  C w = __ldg(&tab[idx]);
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+// One radix-8 pass with Ns > 1 for butterfly j = t on registers v.
+template <typename C>
+__device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
+                                           const C *__restrict__ tab, int sign) {
+  const C w1 = tw_load(tab, k * step, sign);
+  const C w2 = tw_load(tab, 2 * k * step, sign);
+  const C w4 = tw_load(tab, 4 * k * step, sign);
+  const C w3 = cmul(w1, w2);
+  v[1] = cmul(v[1], w1);
+  v[2] = cmul(v[2], w2);
+  v[3] = cmul(v[3], w3);
+  v[4] = cmul(v[4], w4);
+  v[5] = cmul(v[5], cmul(w1, w4));
+  v[6] = cmul(v[6], cmul(w2, w4));
+  v[7] = cmul(v[7], cmul(w3, w4));
+}
+
+// Transform of one column held in registers (layout above).  ex(i) gives the
+// shared-memory slot of row i of this thread's column; all TPC threads of
+// every column in the CTA must call this together.
+template <int L, typename C, typename Ex>
+__device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
+                                        const C *__restrict__ tab, int sign,
+                                        int tab_scale = 1) {
+  constexpr int TPC = L / 8;
+  // Number of radix-8 passes and the leading radix (1, 2 or 4).
+  constexpr int LOG = __builtin_ctz(L);
+  constexpr int P8 = LOG / 3;
+  constexpr int R0 = 1 << (LOG - 3 * P8);
+  int Ns = 1;
+  if constexpr (R0 == 2) {
+    // Four radix-2 butterflies j = t + TPC c, inputs x[j + (L/2) q] = v[c + 4q].
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      C a = v[c], b = v[c + 4];
+      v[c] = cadd(a, b);
+      v[c + 4] = csub(a, b);
+    }
+    // Outputs y[2j + q]: write, then read x[t + TPC u].
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int j = t + TPC * c;
+      *ex(2 * j) = v[c];
+      *ex(2 * j + 1) = v[c + 4];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = *ex(t + TPC * u);
+    __syncthreads();
+    Ns = 2;
+  } else if constexpr (R0 == 4) {
+    // Two radix-4 butterflies j = t + TPC c, inputs x[j + (L/4) q] = v[c + 2q].
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      C w[4] = {v[c], v[c + 2], v[c + 4], v[c + 6]};
+      Dft<4, C>::run(w, sign);
+      v[c] = w[0];
+      v[c + 2] = w[1];
+      v[c + 4] = w[2];
+      v[c + 6] = w[3];
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const int j = t + TPC * c;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) *ex(4 * j + q) = v[c + 2 * q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = *ex(t + TPC * u);
+    __syncthreads();
+    Ns = 4;
+  }
+#pragma unroll
+  for (int p = 0; p < P8; ++p) {
+    const int k = t & (Ns - 1);
+    if (Ns > 1) r8_twiddle(v, k, (L / (8 * Ns)) * tab_scale, tab, sign);
+    Dft<8, C>::run(v, sign);
+    if (p + 1 < P8) {
+      const int o = (t - k) * 8 + k;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) *ex(o + q * Ns) = v[q];
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = *ex(t + TPC * u);
+      __syncthreads();
+    }
+    Ns *= 8;
+  }
 }
 
 }  // namespace fc

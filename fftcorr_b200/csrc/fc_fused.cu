@@ -30,23 +30,48 @@
 namespace fc {
 namespace {
 
-constexpr int kThreads = 256;  // threads per CTA of every fused pass
-
 template <typename T>
 using C2 = typename Vec2<T>::type;
+
+// Columns (or rows) per CTA: 64-byte segments of complex values.
+template <typename T>
+struct Tile {
+  static constexpr int B = 64 / (2 * sizeof(T));  // 8 for FP32, 4 for FP64
+};
+
+// Y_lm * D in the arithmetic of the pass: the reference's FP64 evaluation
+// for the FP64 form, the FP32 evaluator (FP64 coordinates and
+// normalisation) for the FP32-mixed form.
+template <typename T>
+__device__ __forceinline__ T weight_value(const YlmParams &p, T D, double x,
+                                          double y, double z);
+template <>
+__device__ __forceinline__ double weight_value<double>(const YlmParams &p,
+                                                       double D, double x,
+                                                       double y, double z) {
+  return ylm_eval(p, D, x, y, z);
+}
+template <>
+__device__ __forceinline__ float weight_value<float>(const YlmParams &p,
+                                                     float D, double x,
+                                                     double y, double z) {
+  return ylm_eval_f32(p, D, x, y, z);
+}
 
 // ------------------------------------------------------------------ zfwd
 // B rows of N2 reals per CTA: (optionally Y_lm-weighted) packed as
 // z_j = x_2j + i x_2j+1, length-M complex DFT, then the real-to-complex
 // split X_k = E_k + e^{-2 pi i k/N2} O_k for k <= M.
-template <typename T, typename TI, bool WEIGHT>
-__global__ void k_zfwd(const TI *__restrict__ rho, C2<T> *__restrict__ W,
-                       FusedGeom g, YlmParams p, double x0, double y0,
-                       double z0, const C2<T> *__restrict__ tabz, int B) {
+template <typename T, bool WEIGHT>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
+    k_zfwd(const T *__restrict__ rho, C2<T> *__restrict__ W, FusedGeom g,
+           YlmParams p, double x0, double y0, double z0,
+           const C2<T> *__restrict__ tabz) {
   using C = C2<T>;
+  constexpr int B = Tile<T>::B;
+  constexpr int BP = B + 1;
   extern __shared__ unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
-  const int BP = B + 1;
   const int M = g.m;
   C *buf2 = buf + M * BP;
   const int64_t nrows = (int64_t)g.n0 * g.n1;
@@ -59,48 +84,46 @@ __global__ void k_zfwd(const TI *__restrict__ rho, C2<T> *__restrict__ W,
     z.x = 0;
     z.y = 0;
     if (row < nrows) {
-      const TI *src = rho + row * g.n2 + 2 * j;
-      double v0 = (double)src[0];
-      double v1 = (double)src[1];
+      const typename Vec2<T>::type v =
+          reinterpret_cast<const typename Vec2<T>::type *>(rho + row * g.n2)[j];
+      z = v;
       if (WEIGHT) {
         const int x = (int)(row / g.n1);
         const int y = (int)(row - (int64_t)x * g.n1);
         const double cx = x0 + x * 1.0;
         const double cy = y0 + y * 1.0;
-        v0 = ylm_eval(p, v0, cx, cy, z0 + (2 * j) * 1.0);
-        v1 = ylm_eval(p, v1, cx, cy, z0 + (2 * j + 1) * 1.0);
+        z.x = weight_value<T>(p, v.x, cx, cy, z0 + (2 * j) * 1.0);
+        z.y = weight_value<T>(p, v.y, cx, cy, z0 + (2 * j + 1) * 1.0);
       }
-      z.x = (T)v0;
-      z.y = (T)v1;
     }
     buf[j * BP + b] = z;
   }
   __syncthreads();
-  buf = fft_columns(buf, buf2, g.pz, B, BP, tabz, -1);
+  buf = fft_columns<B>(buf, buf2, g.pz, tabz, -1);
   const int H = M + 1;
   for (int idx = threadIdx.x; idx < H * B; idx += blockDim.x) {
     const int b = idx / H;
     const int k = idx - b * H;
     const int64_t row = row0 + b;
     if (row >= nrows) continue;
-    const C a = buf[(k % M) * BP + b];
-    const C c = cconj(buf[((M - k) % M) * BP + b]);
+    const C a = buf[(k == M ? 0 : k) * BP + b];
+    const C c = cconj(buf[(k == 0 ? 0 : M - k) * BP + b]);
     C e, d, o;
     e.x = (T)0.5 * (a.x + c.x);
     e.y = (T)0.5 * (a.y + c.y);
     d = csub(a, c);
     o.x = (T)0.5 * d.y;  // -i (a - c) / 2
     o.y = (T)-0.5 * d.x;
-    W[row * g.h + k] = cadd(e, cmul(tabz[k], o));
+    W[row * g.h + k] = cadd(e, cmul(__ldg(&tabz[k]), o));
   }
 }
 
 // Loads a B-column tile of a strided axis into shared memory.
-template <typename C>
+template <int B, typename C>
 __device__ __forceinline__ void load_columns(C *buf, const C *__restrict__ src,
                                              int64_t base, int64_t stride,
-                                             int L, int B, int BP, int kz0,
-                                             int h) {
+                                             int L, int kz0, int h) {
+  constexpr int BP = B + 1;
   for (int idx = threadIdx.x; idx < L * B; idx += blockDim.x) {
     const int i = idx / B;
     const int b = idx - i * B;
@@ -115,17 +138,18 @@ __device__ __forceinline__ void load_columns(C *buf, const C *__restrict__ src,
 
 // ------------------------------------------------------------------ yfwd
 template <typename T>
-__global__ void k_yfwd(C2<T> *__restrict__ W, FusedGeom g,
-                       const C2<T> *__restrict__ taby, int B) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
+    k_yfwd(C2<T> *__restrict__ W, FusedGeom g, const C2<T> *__restrict__ taby) {
   using C = C2<T>;
+  constexpr int B = Tile<T>::B;
+  constexpr int BP = B + 1;
   extern __shared__ unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
-  const int BP = B + 1;
   const int kz0 = blockIdx.x * B;
   const int x = blockIdx.y;
   const int64_t base = (int64_t)x * g.n1 * g.h;
-  load_columns(buf, W, base, g.h, g.n1, B, BP, kz0, g.h);
-  buf = fft_columns(buf, buf + g.n1 * BP, g.py, B, BP, taby, -1);
+  load_columns<B>(buf, W, base, g.h, g.n1, kz0, g.h);
+  buf = fft_columns<B>(buf, buf + g.n1 * BP, g.py, taby, -1);
   for (int idx = threadIdx.x; idx < g.n1 * B; idx += blockDim.x) {
     const int i = idx / B;
     const int b = idx - i * B;
@@ -137,28 +161,26 @@ __global__ void k_yfwd(C2<T> *__restrict__ W, FusedGeom g,
 // MODE 0: G = DFT_x(W) (grid2's transform).  MODE 1: the fused product,
 // k-subgrid extraction, inverse and pruning described at the top.
 template <typename T, int MODE>
-__global__ void k_xcorr(const C2<T> *__restrict__ W,
-                        const C2<T> *__restrict__ G, C2<T> *__restrict__ out,
-                        double *__restrict__ ksub, FusedGeom g,
-                        const C2<T> *__restrict__ tabx,
-                        const double *__restrict__ kx,
-                        const double *__restrict__ ky,
-                        const double *__restrict__ kz,
-                        const double *__restrict__ wx,
-                        const double *__restrict__ wy,
-                        const double *__restrict__ wz, YlmParams pk, int B) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
+    k_xcorr(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
+            C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
+            const C2<T> *__restrict__ tabx, const double *__restrict__ kx,
+            const double *__restrict__ ky, const double *__restrict__ kz,
+            const double *__restrict__ wx, const double *__restrict__ wy,
+            const double *__restrict__ wz, YlmParams pk) {
   using C = C2<T>;
+  constexpr int B = Tile<T>::B;
+  constexpr int BP = B + 1;
   extern __shared__ unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
-  const int BP = B + 1;
   const int kz0 = blockIdx.x * B;
   const int yy = blockIdx.y;
   const int64_t stride = (int64_t)g.n1 * g.h;
   const int64_t base = (int64_t)yy * g.h;
   C *other = buf + g.n0 * BP;
-  load_columns(buf, W, base, stride, g.n0, B, BP, kz0, g.h);
+  load_columns<B>(buf, W, base, stride, g.n0, kz0, g.h);
   {
-    C *res = fft_columns(buf, other, g.px, B, BP, tabx, -1);
+    C *res = fft_columns<B>(buf, other, g.px, tabx, -1);
     other = res == buf ? other : buf;
     buf = res;
   }
@@ -168,70 +190,73 @@ __global__ void k_xcorr(const C2<T> *__restrict__ W,
       const int b = idx - i * B;
       if (kz0 + b < g.h) out[base + i * stride + kz0 + b] = buf[i * BP + b];
     }
-    return;
   } else {
-  // P = F * conj(G).
-  for (int idx = threadIdx.x; idx < g.n0 * B; idx += blockDim.x) {
-    const int i = idx / B;
-    const int b = idx - i * B;
-    if (kz0 + b < g.h)
-      buf[i * BP + b] = cmulc(buf[i * BP + b], G[base + i * stride + kz0 + b]);
-  }
-  __syncthreads();
-  // k-subgrid: this CTA owns the sources with ky index yy and kz in its
-  // block.  Direct targets k = kz + oz read P[(i - ox) mod N0][yy][kz];
-  // reflected targets k = oz - kz (kz >= 1) read P[(ox - i) mod N0][yy][kz]
-  // for j with (oy - j) mod N1 == yy.  Every ksub cell has exactly one
-  // source element, so these read-modify-writes never collide.
-  if (ksub != nullptr) {
-    const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
-    for (int refl = 0; refl < 2; ++refl) {
-      int j = refl == 0 ? (yy + oy) % g.n1 : ((oy - yy) % g.n1 + g.n1) % g.n1;
-      for (; j < g.ks1; j += g.n1) {
-        for (int idx = threadIdx.x; idx < g.ks0 * B; idx += blockDim.x) {
-          const int i = idx / B;
-          const int b = idx - i * B;
-          const int kzi = kz0 + b;
-          if (kzi >= g.h || kzi > oz || (refl == 1 && kzi == 0)) continue;
-          const int k = refl == 0 ? kzi + oz : oz - kzi;
-          const int x = refl == 0 ? ((i - ox) % g.n0 + g.n0) % g.n0
-                                  : ((ox - i) % g.n0 + g.n0) % g.n0;
-          const double re = (double)buf[x * BP + b].x;
-          const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
-          const double yv = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
-          double *dst = ksub + ((size_t)i * g.ks1 + j) * g.ks2 + k;
-          *dst += yv * re;
-        }
-      }
+    // P = F * conj(G).
+    for (int idx = threadIdx.x; idx < g.n0 * B; idx += blockDim.x) {
+      const int i = idx / B;
+      const int b = idx - i * B;
+      if (kz0 + b < g.h)
+        buf[i * BP + b] = cmulc(buf[i * BP + b], G[base + i * stride + kz0 + b]);
     }
     __syncthreads();
-  }
-  buf = fft_columns(buf, other, g.px, B, BP, tabx, +1);
-  const int64_t obase = (int64_t)yy * g.h;
-  const int64_t ostride = (int64_t)g.n1 * g.h;
-  for (int idx = threadIdx.x; idx < g.rs * B; idx += blockDim.x) {
-    const int ri = idx / B;
-    const int b = idx - ri * B;
-    if (kz0 + b >= g.h) continue;
-    const int x = ((ri - g.ro) % g.n0 + g.n0) % g.n0;
-    out[obase + ri * ostride + kz0 + b] = buf[x * BP + b];
-  }
+    // k-subgrid: this CTA owns the sources with ky index yy and kz in its
+    // block.  Direct targets k = kz + oz read P[(i - ox) mod N0][yy][kz];
+    // reflected targets k = oz - kz (kz >= 1) read P[(ox - i) mod N0][yy][kz]
+    // for j with (oy - j) mod N1 == yy.  Every ksub cell has exactly one
+    // source element, so these read-modify-writes never collide.
+    if (ksub != nullptr) {
+      const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
+      if (kz0 <= oz) {
+        for (int refl = 0; refl < 2; ++refl) {
+          int j = refl == 0 ? (yy + oy) % g.n1 : ((oy - yy) % g.n1 + g.n1) % g.n1;
+          for (; j < g.ks1; j += g.n1) {
+            for (int idx = threadIdx.x; idx < g.ks0 * B; idx += blockDim.x) {
+              const int i = idx / B;
+              const int b = idx - i * B;
+              const int kzi = kz0 + b;
+              if (kzi >= g.h || kzi > oz || (refl == 1 && kzi == 0)) continue;
+              const int k = refl == 0 ? kzi + oz : oz - kzi;
+              const int x = refl == 0 ? ((i - ox) % g.n0 + g.n0) % g.n0
+                                      : ((ox - i) % g.n0 + g.n0) % g.n0;
+              const double re = (double)buf[x * BP + b].x;
+              const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
+              const double yv = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
+              double *dst = ksub + ((size_t)i * g.ks1 + j) * g.ks2 + k;
+              *dst += yv * re;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    buf = fft_columns<B>(buf, other, g.px, tabx, +1);
+    const int64_t obase = (int64_t)yy * g.h;
+    const int64_t ostride = (int64_t)g.n1 * g.h;
+    for (int idx = threadIdx.x; idx < g.rs * B; idx += blockDim.x) {
+      const int ri = idx / B;
+      const int b = idx - ri * B;
+      if (kz0 + b >= g.h) continue;
+      const int x = ((ri - g.ro) % g.n0 + g.n0) % g.n0;
+      out[obase + ri * ostride + kz0 + b] = buf[x * BP + b];
+    }
   }
 }
 
 // ------------------------------------------------------------------ yinv
 template <typename T>
-__global__ void k_yinv(const C2<T> *__restrict__ Wr, C2<T> *__restrict__ Wry,
-                       FusedGeom g, const C2<T> *__restrict__ taby, int B) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
+    k_yinv(const C2<T> *__restrict__ Wr, C2<T> *__restrict__ Wry, FusedGeom g,
+           const C2<T> *__restrict__ taby) {
   using C = C2<T>;
+  constexpr int B = Tile<T>::B;
+  constexpr int BP = B + 1;
   extern __shared__ unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
-  const int BP = B + 1;
   const int kz0 = blockIdx.x * B;
   const int ri = blockIdx.y;
   const int64_t base = (int64_t)ri * g.n1 * g.h;
-  load_columns(buf, Wr, base, g.h, g.n1, B, BP, kz0, g.h);
-  buf = fft_columns(buf, buf + g.n1 * BP, g.py, B, BP, taby, +1);
+  load_columns<B>(buf, Wr, base, g.h, g.n1, kz0, g.h);
+  buf = fft_columns<B>(buf, buf + g.n1 * BP, g.py, taby, +1);
   const int64_t obase = (int64_t)ri * g.rs * g.h;
   for (int idx = threadIdx.x; idx < g.rs * B; idx += blockDim.x) {
     const int rj = idx / B;
@@ -247,15 +272,15 @@ __global__ void k_yinv(const C2<T> *__restrict__ Wr, C2<T> *__restrict__ Wry,
 // the imaginary parts of the DC and Nyquist terms ignored), then
 // rsub[ri][rj][rk] += Y_lm(r) * value at z = (N2 - rs/2 + rk) mod N2.
 template <typename T>
-__global__ void k_zinv_rsub(const C2<T> *__restrict__ Wry,
-                            double *__restrict__ rsub, FusedGeom g,
-                            const C2<T> *__restrict__ tabz,
-                            const double *__restrict__ raxis, YlmParams pr,
-                            int B) {
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
+    k_zinv_rsub(const C2<T> *__restrict__ Wry, double *__restrict__ rsub,
+                FusedGeom g, const C2<T> *__restrict__ tabz,
+                const double *__restrict__ raxis, YlmParams pr) {
   using C = C2<T>;
+  constexpr int B = Tile<T>::B;
+  constexpr int BP = B + 1;
   extern __shared__ unsigned char smem_raw[];
   C *buf = reinterpret_cast<C *>(smem_raw);
-  const int BP = B + 1;
   const int M = g.m;
   const int nrows = g.rs * g.rs;
   const int row0 = blockIdx.x * B;
@@ -276,14 +301,14 @@ __global__ void k_zinv_rsub(const C2<T> *__restrict__ Wry,
         c.y = 0;  // X[M] is the Nyquist term
       }
       const C e = cadd(a, c);
-      const C o = cmul(csub(a, c), cconj(tabz[k]));  // times e^{+2 pi i k/N2}
+      const C o = cmul(csub(a, c), cconj(__ldg(&tabz[k])));  // e^{+2 pi i k/N2}
       z.x = e.x - o.y;
       z.y = e.y + o.x;
     }
     buf[k * BP + b] = z;
   }
   __syncthreads();
-  buf = fft_columns(buf, buf2, g.pz, B, BP, tabz, +1);
+  buf = fft_columns<B>(buf, buf2, g.pz, tabz, +1);
   for (int idx = threadIdx.x; idx < g.rs * B; idx += blockDim.x) {
     const int b = idx / g.rs;
     const int rk = idx - b * g.rs;
@@ -296,6 +321,271 @@ __global__ void k_zinv_rsub(const C2<T> *__restrict__ Wry,
     const double v = (double)((z & 1) ? zz.y : zz.x);
     const double yv = ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
     rsub[(size_t)row * g.rs + rk] += yv * v;
+  }
+}
+
+// --------------------------------------------------------------------------
+// Power-of-two lengths: the same passes with the register-resident engine
+// (reg_fft in fc_fft.cuh).  B2 columns per CTA keep the CTA at <= 1024
+// threads (TPC = L/8 threads per column).
+template <typename T, int L>
+struct P2 {
+  static constexpr int B = (Tile<T>::B < 8192 / L) ? Tile<T>::B : 8192 / L;
+  static constexpr int TPC = L / 8;
+  static constexpr int THREADS = TPC * B;
+  static constexpr int BP = B + 1;
+};
+
+template <typename T, int L>
+__global__ void __launch_bounds__(P2<T, L>::THREADS)
+    k_yfwd_p2(C2<T> *__restrict__ W, FusedGeom g,
+              const C2<T> *__restrict__ taby) {
+  using C = C2<T>;
+  using Q = P2<T, L>;
+  extern __shared__ unsigned char smem_raw[];
+  C *ex = reinterpret_cast<C *>(smem_raw);
+  const int t = threadIdx.x / Q::B;
+  const int b = threadIdx.x - t * Q::B;
+  const int kz0 = blockIdx.x * Q::B;
+  const bool valid = kz0 + b < g.h;
+  const int64_t base = (int64_t)blockIdx.y * L * g.h + kz0 + b;
+  C v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    v[u].x = 0;
+    v[u].y = 0;
+    if (valid) v[u] = W[base + (int64_t)(t + Q::TPC * u) * g.h];
+  }
+  reg_fft<L>(v, t, [&](int i) { return &ex[i * Q::BP + b]; }, taby, -1);
+  if (valid) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) W[base + (int64_t)(t + Q::TPC * u) * g.h] = v[u];
+  }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(P2<T, L>::THREADS)
+    k_yinv_p2(const C2<T> *__restrict__ Wr, C2<T> *__restrict__ Wry,
+              FusedGeom g, const C2<T> *__restrict__ taby) {
+  using C = C2<T>;
+  using Q = P2<T, L>;
+  extern __shared__ unsigned char smem_raw[];
+  C *ex = reinterpret_cast<C *>(smem_raw);
+  const int t = threadIdx.x / Q::B;
+  const int b = threadIdx.x - t * Q::B;
+  const int kz0 = blockIdx.x * Q::B;
+  const int ri = blockIdx.y;
+  const bool valid = kz0 + b < g.h;
+  const int64_t base = (int64_t)ri * L * g.h + kz0 + b;
+  C v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    v[u].x = 0;
+    v[u].y = 0;
+    if (valid) v[u] = Wr[base + (int64_t)(t + Q::TPC * u) * g.h];
+  }
+  reg_fft<L>(v, t, [&](int i) { return &ex[i * Q::BP + b]; }, taby, +1);
+  if (!valid) return;
+  const int64_t obase = (int64_t)ri * g.rs * g.h + kz0 + b;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int y = t + Q::TPC * u;
+    for (int rj = (y + g.ro) % L; rj < g.rs; rj += L)
+      Wry[obase + (int64_t)rj * g.h] = v[u];
+  }
+}
+
+template <typename T, int L, int MODE>
+__global__ void __launch_bounds__(P2<T, L>::THREADS)
+    k_xcorr_p2(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
+               C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
+               const C2<T> *__restrict__ tabx, const double *__restrict__ kx,
+               const double *__restrict__ ky, const double *__restrict__ kz,
+               const double *__restrict__ wx, const double *__restrict__ wy,
+               const double *__restrict__ wz, YlmParams pk) {
+  using C = C2<T>;
+  using Q = P2<T, L>;
+  extern __shared__ unsigned char smem_raw[];
+  C *ex = reinterpret_cast<C *>(smem_raw);
+  const int t = threadIdx.x / Q::B;
+  const int b = threadIdx.x - t * Q::B;
+  const int kz0 = blockIdx.x * Q::B;
+  const int yy = blockIdx.y;
+  const int kzi = kz0 + b;
+  const bool valid = kzi < g.h;
+  const int64_t stride = (int64_t)g.n1 * g.h;
+  const int64_t base = (int64_t)yy * g.h + kzi;
+  auto exf = [&](int i) { return &ex[i * Q::BP + b]; };
+  C v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    v[u].x = 0;
+    v[u].y = 0;
+    if (valid) v[u] = W[base + (t + Q::TPC * u) * stride];
+  }
+  reg_fft<L>(v, t, exf, tabx, -1);
+  if constexpr (MODE == 0) {
+    if (valid) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) out[base + (t + Q::TPC * u) * stride] = v[u];
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (valid) v[u] = cmulc(v[u], G[base + (t + Q::TPC * u) * stride]);
+    // k-subgrid extraction (see k_xcorr): needs P at arbitrary rows.
+    const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
+    if (ksub != nullptr && kz0 <= oz) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
+      __syncthreads();
+      if (valid && kzi <= oz) {
+        for (int refl = 0; refl < 2; ++refl) {
+          if (refl == 1 && kzi == 0) continue;
+          const int k = refl == 0 ? kzi + oz : oz - kzi;
+          int j = refl == 0 ? (yy + oy) % g.n1 : ((oy - yy) % g.n1 + g.n1) % g.n1;
+          for (; j < g.ks1; j += g.n1) {
+            for (int i = t; i < g.ks0; i += Q::TPC) {
+              const int x = refl == 0 ? ((i - ox) % L + L) % L
+                                      : ((ox - i) % L + L) % L;
+              const double re = (double)exf(x)->x;
+              const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
+              const double yv = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
+              double *dst = ksub + ((size_t)i * g.ks1 + j) * g.ks2 + k;
+              *dst += yv * re;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    reg_fft<L>(v, t, exf, tabx, +1);
+    if (valid) {
+      const int64_t obase = (int64_t)yy * g.h + kzi;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int x = t + Q::TPC * u;
+        for (int ri = (x + g.ro) % L; ri < g.rs; ri += L)
+          out[obase + ri * stride] = v[u];
+      }
+    }
+  }
+}
+
+// Rows of the z transform: thread t of row b holds z[t + TPC u].
+template <typename T, int L, bool WEIGHT>
+__global__ void __launch_bounds__(P2<T, L>::THREADS)
+    k_zfwd_p2(const T *__restrict__ rho, C2<T> *__restrict__ W, FusedGeom g,
+              YlmParams p, double x0, double y0, double z0,
+              const C2<T> *__restrict__ tabz) {
+  using C = C2<T>;
+  using Q = P2<T, L>;
+  // Row pitch in shared memory, with one pad slot every 8 elements so the
+  // strided Stockham writes spread over the banks.
+  constexpr int RP = L + L / 8 + 1;
+  extern __shared__ unsigned char smem_raw[];
+  C *ex = reinterpret_cast<C *>(smem_raw);
+  const int b = threadIdx.x / Q::TPC;
+  const int t = threadIdx.x - b * Q::TPC;
+  const int64_t nrows = (int64_t)g.n0 * g.n1;
+  const int64_t row = (int64_t)blockIdx.x * Q::B + b;
+  const bool valid = row < nrows;
+  C v[8];
+  int x = 0, y = 0;
+  if (valid) {
+    x = (int)(row / g.n1);
+    y = (int)(row - (int64_t)x * g.n1);
+  }
+  const double cx = x0 + x * 1.0;
+  const double cy = y0 + y * 1.0;
+  const C *src = reinterpret_cast<const C *>(rho + row * g.n2);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    v[u].x = 0;
+    v[u].y = 0;
+    if (valid) {
+      const int jj = t + Q::TPC * u;
+      const C pr = src[jj];
+      v[u] = pr;
+      if (WEIGHT) {
+        v[u].x = weight_value<T>(p, pr.x, cx, cy, z0 + (2 * jj) * 1.0);
+        v[u].y = weight_value<T>(p, pr.y, cx, cy, z0 + (2 * jj + 1) * 1.0);
+      }
+    }
+  }
+  auto exf = [&](int i) { return &ex[b * RP + i + (i >> 3)]; };
+  reg_fft<L>(v, t, exf, tabz, -1, 2);
+  // Real-to-complex split needs Z_k and Z_{M-k}.
+#pragma unroll
+  for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
+  __syncthreads();
+  if (!valid) return;
+  C *dst = W + row * g.h;
+  for (int k = t; k <= L; k += Q::TPC) {
+    const C a = *exf(k == L ? 0 : k);
+    const C c = cconj(*exf(k == 0 ? 0 : L - k));
+    C e, d, o;
+    e.x = (T)0.5 * (a.x + c.x);
+    e.y = (T)0.5 * (a.y + c.y);
+    d = csub(a, c);
+    o.x = (T)0.5 * d.y;
+    o.y = (T)-0.5 * d.x;
+    dst[k] = cadd(e, cmul(__ldg(&tabz[k]), o));
+  }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(P2<T, L>::THREADS)
+    k_zinv_p2(const C2<T> *__restrict__ Wry, double *__restrict__ rsub,
+              FusedGeom g, const C2<T> *__restrict__ tabz,
+              const double *__restrict__ raxis, YlmParams pr) {
+  using C = C2<T>;
+  using Q = P2<T, L>;
+  constexpr int RP = L + L / 8 + 1;
+  extern __shared__ unsigned char smem_raw[];
+  C *ex = reinterpret_cast<C *>(smem_raw);
+  const int b = threadIdx.x / Q::TPC;
+  const int t = threadIdx.x - b * Q::TPC;
+  const int nrows = g.rs * g.rs;
+  const int row = blockIdx.x * Q::B + b;
+  const bool valid = row < nrows;
+  C v[8];
+  const C *X = Wry + (int64_t)(valid ? row : 0) * g.h;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int k = t + Q::TPC * u;
+    v[u].x = 0;
+    v[u].y = 0;
+    if (valid) {
+      C a = X[k];
+      C c = cconj(X[L - k]);
+      if (k == 0) {
+        a.y = 0;
+        c.y = 0;
+      }
+      const C e = cadd(a, c);
+      const C o = cmul(csub(a, c), cconj(__ldg(&tabz[k])));
+      v[u].x = e.x - o.y;
+      v[u].y = e.y + o.x;
+    }
+  }
+  auto exf = [&](int i) { return &ex[b * RP + i + (i >> 3)]; };
+  reg_fft<L>(v, t, exf, tabz, +1, 2);
+  if (!valid) return;
+  const int ri = row / g.rs;
+  const int rj = row - ri * g.rs;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int jj = t + Q::TPC * u;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int z = 2 * jj + h;
+      const double val = (double)(h ? v[u].y : v[u].x);
+      for (int rk = (z + g.ro) % g.n2; rk < g.rs; rk += g.n2) {
+        const double yv = ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
+        rsub[(size_t)row * g.rs + rk] += yv * val;
+      }
+    }
   }
 }
 
@@ -325,6 +615,7 @@ bool plan_length(int L, int tab_scale, FftPlan *p) {
   int ns = 1;
   for (int s = 0; s < p->npass; ++s) {
     p->ns[s] = ns;
+    p->nsmask[s] = (ns & (ns - 1)) == 0 ? ns - 1 : -1;
     ns *= p->radix[s];
   }
   return true;
@@ -342,13 +633,57 @@ std::vector<C> root_table(int order) {
   return t;
 }
 
-int cols_for(int L, int elem_bytes) {
-  // Columns per CTA: 64-byte row segments (full 32-byte sectors) while the
-  // two shared-memory tiles (2 x L x (B+1) complex) stay within 100 KB, so
-  // two or more CTAs fit on an SM.
-  int B = 64 / elem_bytes;
-  while (B > 1 && 2 * (size_t)L * (B + 1) * elem_bytes > 100 * 1024) B /= 2;
-  return B;
+// Threads per CTA for a pass of length L over B columns: one thread per
+// radix-8 butterfly where possible, between 128 and 256.
+int threads_for(int L, int B) {
+  int t = (L / 8) * B;
+  t = ((t + 31) / 32) * 32;
+  return std::max(128, std::min(256, t));
+}
+
+// ----------------------------------------------------- power-of-two dispatch
+
+bool is_p2(int L) { return L >= 64 && L <= 2048 && (L & (L - 1)) == 0; }
+
+template <typename T, int L>
+size_t p2_col_smem() {
+  return (size_t)L * P2<T, L>::BP * sizeof(C2<T>);
+}
+template <typename T, int L>
+size_t p2_row_smem() {
+  return (size_t)P2<T, L>::B * (L + L / 8 + 1) * sizeof(C2<T>);
+}
+
+// Calls f.template operator()<L>() for the power-of-two L.
+template <typename F>
+void with_p2(int L, F &&f) {
+  switch (L) {
+    case 64: f.template operator()<64>(); break;
+    case 128: f.template operator()<128>(); break;
+    case 256: f.template operator()<256>(); break;
+    case 512: f.template operator()<512>(); break;
+    case 1024: f.template operator()<1024>(); break;
+    default: f.template operator()<2048>(); break;
+  }
+}
+
+template <typename T, int L>
+void p2_set_limits() {
+  const int big = 200 * 1024;
+  FC_CUDA(cudaFuncSetAttribute(k_yfwd_p2<T, L>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_yinv_p2<T, L>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_xcorr_p2<T, L, 0>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_xcorr_p2<T, L, 1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_zfwd_p2<T, L, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_zfwd_p2<T, L, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_zinv_p2<T, L>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
 }
 
 }  // namespace
@@ -359,9 +694,11 @@ bool FusedSurvey::supported(const int shape[3], int rsize) {
   if (!plan_length(shape[0], 1, &p) || !plan_length(shape[1], 1, &p) ||
       !plan_length(shape[2] / 2, 2, &p))
     return false;
+  // Two shared tiles of L x (B+1) complex must fit in 200 KB.
   for (int a = 0; a < 3; ++a) {
     const int L = a == 2 ? shape[2] / 2 : shape[a];
-    if (L > 4096) return false;
+    if (2 * (size_t)L * 5 * 16 > 200 * 1024 || 2 * (size_t)L * 9 * 8 > 200 * 1024)
+      return false;
   }
   return rsize > 0;
 }
@@ -384,21 +721,14 @@ FusedSurvey::FusedSurvey(const int shape[3], int rsize, const int kshape[3],
              FC_ERR_UNSUPPORTED, "grid size has a prime factor above 7");
   const size_t eb = fp64 ? 16 : 8;
   if (fp64) {
-    auto tx = root_table<double2>(g.n0), ty = root_table<double2>(g.n1),
-         tz = root_table<double2>(g.n2);
-    upload(tabx, tx);
-    upload(taby, ty);
-    upload(tabz, tz);
+    upload(tabx, root_table<double2>(g.n0));
+    upload(taby, root_table<double2>(g.n1));
+    upload(tabz, root_table<double2>(g.n2));
   } else {
-    auto tx = root_table<float2>(g.n0), ty = root_table<float2>(g.n1),
-         tz = root_table<float2>(g.n2);
-    upload(tabx, tx);
-    upload(taby, ty);
-    upload(tabz, tz);
+    upload(tabx, root_table<float2>(g.n0));
+    upload(taby, root_table<float2>(g.n1));
+    upload(tabz, root_table<float2>(g.n2));
   }
-  bx = cols_for(g.n0, (int)eb);
-  by = cols_for(g.n1, (int)eb);
-  bz = cols_for(g.m, (int)eb);
   const size_t nc = (size_t)g.n0 * g.n1 * g.h;
   W.resize(nc * eb);
   G.resize(nc * eb);
@@ -415,42 +745,41 @@ void FusedSurvey::upload(DeviceBuffer &dst, const std::vector<V> &v) {
                      cudaMemcpyHostToDevice));
 }
 
-size_t FusedSurvey::smem(int L, int B) const {
+size_t FusedSurvey::smem(int L) const {
+  const int B = fp64_ ? Tile<double>::B : Tile<float>::B;
   return 2 * (size_t)L * (B + 1) * (fp64_ ? 16 : 8);
 }
 
-void FusedSurvey::set_smem_limits() {
+template <typename T>
+static void set_limits_for() {
   const int big = 200 * 1024;
-  if (fp64_) {
-    FC_CUDA(cudaFuncSetAttribute(k_zfwd<double, double, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_zfwd<double, double, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_yfwd<double>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_xcorr<double, 0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_xcorr<double, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_yinv<double>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_zinv_rsub<double>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  } else {
-    FC_CUDA(cudaFuncSetAttribute(k_zfwd<float, float, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_zfwd<float, float, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_yfwd<float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_xcorr<float, 0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_xcorr<float, 1>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_yinv<float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-    FC_CUDA(cudaFuncSetAttribute(k_zinv_rsub<float>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_zfwd<T, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_zfwd<T, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_yfwd<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_xcorr<T, 0>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_xcorr<T, 1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_yinv<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_zinv_rsub<T>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+}
+
+void FusedSurvey::set_smem_limits() {
+  if (fp64_)
+    set_limits_for<double>();
+  else
+    set_limits_for<float>();
+  for (int L : {g.n0, g.n1, g.m}) {
+    if (!is_p2(L)) continue;
+    if (fp64_)
+      with_p2(L, [&]<int LL>() { p2_set_limits<double, LL>(); });
+    else
+      with_p2(L, [&]<int LL>() { p2_set_limits<float, LL>(); });
   }
 }
 
@@ -465,67 +794,131 @@ const void *FusedSurvey::prepare_input(const double *rho, cudaStream_t s) {
 template <typename T>
 void FusedSurvey::zfwd(const void *rho, bool weight, const YlmParams &p,
                        const double xyz0[3], cudaStream_t s) {
-  const int B = bz;
+  if (is_p2(g.m)) {
+    with_p2(g.m, [&]<int L>() {
+      using Q = P2<T, L>;
+      const int64_t nrows = (int64_t)g.n0 * g.n1;
+      const unsigned blocks = (unsigned)((nrows + Q::B - 1) / Q::B);
+      if (weight)
+        k_zfwd_p2<T, L, true><<<blocks, Q::THREADS, p2_row_smem<T, L>(), s>>>(
+            (const T *)rho, W.as<C2<T>>(), g, p, xyz0[0], xyz0[1], xyz0[2],
+            tabz.as<C2<T>>());
+      else
+        k_zfwd_p2<T, L, false><<<blocks, Q::THREADS, p2_row_smem<T, L>(), s>>>(
+            (const T *)rho, W.as<C2<T>>(), g, p, xyz0[0], xyz0[1], xyz0[2],
+            tabz.as<C2<T>>());
+    });
+    FC_LAUNCH_CHECK();
+    return;
+  }
+  constexpr int B = Tile<T>::B;
   const int64_t nrows = (int64_t)g.n0 * g.n1;
   const unsigned blocks = (unsigned)((nrows + B - 1) / B);
-  const int threads = kThreads;
-  const size_t sm = smem(g.m, B);
+  const int threads = threads_for(g.m, B);
+  const size_t sm = smem(g.m);
   if (weight)
-    k_zfwd<T, T, true><<<blocks, threads, sm, s>>>(
+    k_zfwd<T, true><<<blocks, threads, sm, s>>>(
         (const T *)rho, W.as<C2<T>>(), g, p, xyz0[0], xyz0[1], xyz0[2],
-        tabz.as<C2<T>>(), B);
+        tabz.as<C2<T>>());
   else
-    k_zfwd<T, T, false><<<blocks, threads, sm, s>>>(
+    k_zfwd<T, false><<<blocks, threads, sm, s>>>(
         (const T *)rho, W.as<C2<T>>(), g, p, xyz0[0], xyz0[1], xyz0[2],
-        tabz.as<C2<T>>(), B);
+        tabz.as<C2<T>>());
   FC_LAUNCH_CHECK();
 }
 
 template <typename T>
 void FusedSurvey::yfwd(cudaStream_t s) {
-  const int B = by;
+  if (is_p2(g.n1)) {
+    with_p2(g.n1, [&]<int L>() {
+      using Q = P2<T, L>;
+      dim3 grid((g.h + Q::B - 1) / Q::B, g.n0);
+      k_yfwd_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+          W.as<C2<T>>(), g, taby.as<C2<T>>());
+    });
+    FC_LAUNCH_CHECK();
+    return;
+  }
+  constexpr int B = Tile<T>::B;
   dim3 grid((g.h + B - 1) / B, g.n0);
-  k_yfwd<T><<<grid, kThreads, smem(g.n1, B), s>>>(W.as<C2<T>>(), g,
-                                                       taby.as<C2<T>>(), B);
+  k_yfwd<T><<<grid, threads_for(g.n1, B), smem(g.n1), s>>>(W.as<C2<T>>(), g,
+                                                           taby.as<C2<T>>());
   FC_LAUNCH_CHECK();
 }
 
 template <typename T>
 void FusedSurvey::xcorr(bool product, double *ksub, const KAxes &ka,
                         const YlmParams &pk, cudaStream_t s) {
-  const int B = bx;
+  if (is_p2(g.n0)) {
+    with_p2(g.n0, [&]<int L>() {
+      using Q = P2<T, L>;
+      dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
+      if (!product)
+        k_xcorr_p2<T, L, 0><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+            W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
+            ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
+      else
+        k_xcorr_p2<T, L, 1><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+            W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g,
+            tabx.as<C2<T>>(), ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
+    });
+    FC_LAUNCH_CHECK();
+    return;
+  }
+  constexpr int B = Tile<T>::B;
   dim3 grid((g.h + B - 1) / B, g.n1);
-  const int threads = kThreads;
-  const size_t sm = smem(g.n0, B);
+  const int threads = threads_for(g.n0, B);
+  const size_t sm = smem(g.n0);
   if (!product) {
     k_xcorr<T, 0><<<grid, threads, sm, s>>>(
         W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
-        ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk, B);
+        ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
   } else {
     k_xcorr<T, 1><<<grid, threads, sm, s>>>(
         W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g, tabx.as<C2<T>>(),
-        ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk, B);
+        ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
   }
   FC_LAUNCH_CHECK();
 }
 
 template <typename T>
 void FusedSurvey::yinv(cudaStream_t s) {
-  const int B = by;
+  if (is_p2(g.n1)) {
+    with_p2(g.n1, [&]<int L>() {
+      using Q = P2<T, L>;
+      dim3 grid((g.h + Q::B - 1) / Q::B, g.rs);
+      k_yinv_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+          Wr.as<C2<T>>(), Wry.as<C2<T>>(), g, taby.as<C2<T>>());
+    });
+    FC_LAUNCH_CHECK();
+    return;
+  }
+  constexpr int B = Tile<T>::B;
   dim3 grid((g.h + B - 1) / B, g.rs);
-  k_yinv<T><<<grid, kThreads, smem(g.n1, B), s>>>(
-      Wr.as<C2<T>>(), Wry.as<C2<T>>(), g, taby.as<C2<T>>(), B);
+  k_yinv<T><<<grid, threads_for(g.n1, B), smem(g.n1), s>>>(
+      Wr.as<C2<T>>(), Wry.as<C2<T>>(), g, taby.as<C2<T>>());
   FC_LAUNCH_CHECK();
 }
 
 template <typename T>
 void FusedSurvey::zinv(double *rsub, const double *raxis, const YlmParams &pr,
                        cudaStream_t s) {
-  const int B = bz;
+  if (is_p2(g.m)) {
+    with_p2(g.m, [&]<int L>() {
+      using Q = P2<T, L>;
+      const int nrows = g.rs * g.rs;
+      const unsigned blocks = (unsigned)((nrows + Q::B - 1) / Q::B);
+      k_zinv_p2<T, L><<<blocks, Q::THREADS, p2_row_smem<T, L>(), s>>>(
+          Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), raxis, pr);
+    });
+    FC_LAUNCH_CHECK();
+    return;
+  }
+  constexpr int B = Tile<T>::B;
   const int nrows = g.rs * g.rs;
   const unsigned blocks = (unsigned)((nrows + B - 1) / B);
-  k_zinv_rsub<T><<<blocks, kThreads, smem(g.m, B), s>>>(
-      Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), raxis, pr, B);
+  k_zinv_rsub<T><<<blocks, threads_for(g.m, B), smem(g.m), s>>>(
+      Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), raxis, pr);
   FC_LAUNCH_CHECK();
 }
 

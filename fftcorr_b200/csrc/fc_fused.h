@@ -59,7 +59,7 @@ class FusedSurvey {
  private:
   template <typename V>
   void upload(DeviceBuffer &dst, const std::vector<V> &v);
-  size_t smem(int L, int B) const;
+  size_t smem(int L) const;
   void set_smem_limits();
   template <typename T>
   void zfwd(const void *rho, bool weight, const YlmParams &p,
@@ -76,7 +76,6 @@ class FusedSurvey {
             cudaStream_t s);
 
   bool fp64_;
-  int bx = 1, by = 1, bz = 1;  // columns per CTA of each axis
   DeviceBuffer tabx, taby, tabz;
   DeviceBuffer W, G, Wr, Wry, rho32;
 };
