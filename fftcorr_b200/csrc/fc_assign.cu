@@ -11,11 +11,14 @@
 //   K-sort    CUB radix sort of (key, particle index): stable, so the order
 //             of particles inside a cell is their input order
 //   K-tiles   first sorted position of every 8x8x8 tile (binary search)
-//   K-scatter one CTA per tile: particles of the tile are staged in shared
-//             memory with their 1-D stencil weights; every cell of the
-//             tile's footprint (tile + stencil halo) sums its contributions
-//             in a fixed order (home cell, then sorted particle order) and
-//             adds the total to the grid once.  Tiles are processed in colour
+//   K-scatter one CTA per tile.  NGP/CIC/TSC: a thread per home cell sums
+//             its particles' stencil products in registers, and every cell
+//             of the tile's footprint (tile + stencil halo) adds the home
+//             cells' sums in a fixed order.  D12 (8^3 taps): particles are
+//             staged in shared memory with their 1-D weights and every
+//             footprint cell sums its contributions in a fixed order (home
+//             cell, then sorted particle order).  Either way each footprint
+//             total is added to the grid once.  Tiles are processed in colour
 //             passes chosen so that footprints within one pass never
 //             overlap, so there are no atomics and the result is
 //             bit-reproducible run to run.
@@ -350,6 +353,130 @@ __global__ void __launch_bounds__(kScatterThreads)
   }
 }
 
+// K-scatter for stencils of width <= 3 (NGP, CIC, TSC): one thread per
+// home cell of the 8x8x8 tile.  Each thread walks its cell's particles in
+// sorted order and accumulates the W^3 products wx[a]*wy[b]*wz[c] of every
+// particle in registers (S_h[a][b][c]); the sums go to shared memory, and
+// every footprint cell then adds the S_h[o] of the home cells h = f - o in a
+// fixed order.  Per particle this is one gather of its position and W^3
+// register operations, instead of W^3 shared-memory walks.
+template <int S, typename KeyT>
+__global__ void __launch_bounds__(kTileCells)
+    k_scatter_s(const double *__restrict__ posw, const KeyT *__restrict__ keys,
+                const uint32_t *__restrict__ vals,
+                const uint32_t *__restrict__ tile_start,
+                const uint32_t *__restrict__ tiles, AssignGeom g,
+                double *__restrict__ grid) {
+  constexpr int W = Stencil<S>::W;
+  constexpr int OMIN = Stencil<S>::OMIN;
+  constexpr int W3 = W * W * W;
+  constexpr int F = kTile + W - 1;
+  constexpr int F3 = F * F * F;
+  extern __shared__ double smem[];
+  double *sh = smem;              // [W3][512]
+  double *acc = smem + W3 * kTileCells;  // [F3]
+
+  const uint32_t tile = tiles[blockIdx.x];
+  const uint32_t ts = tile_start[tile];
+  const uint32_t te = tile_start[tile + 1];
+  if (ts >= te) return;
+  const int tz = tile % g.nt[2];
+  const int ty = (tile / g.nt[2]) % g.nt[1];
+  const int tx = tile / (g.nt[2] * g.nt[1]);
+  const int o0 = tx * kTile, o1 = ty * kTile, o2 = tz * kTile;
+
+  // This thread's home cell and its particle range [cs, ce).
+  const int h = threadIdx.x;
+  const KeyT kbase = (KeyT)tile * kTileCells;
+  uint32_t lo = ts, hi = te;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (keys[mid] < kbase + h) lo = mid + 1; else hi = mid;
+  }
+  const uint32_t cs = lo;
+  hi = te;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (keys[mid] < kbase + h + 1) lo = mid + 1; else hi = mid;
+  }
+  const uint32_t ce = lo;
+  double sacc[W3];
+#pragma unroll
+  for (int o = 0; o < W3; ++o) sacc[o] = 0.0;
+  for (uint32_t q = cs; q < ce; ++q) {
+    const double *p = posw + 4 * (size_t)vals[q];
+    double x[3];
+    dev_grid_coords(p, g, x);
+    const int ix = home_cell(x[0], g.n[0]);
+    const int iy = home_cell(x[1], g.n[1]);
+    const int iz = home_cell(x[2], g.n[2]);
+    double wx[W], wy[W], wz[W];
+    Stencil<S>::weights(x[0] - ix, x[1] - iy, x[2] - iz, p[3], wx, wy, wz);
+#pragma unroll
+    for (int a = 0; a < W; ++a)
+#pragma unroll
+      for (int b = 0; b < W; ++b) {
+        const double wxy = wx[a] * wy[b];
+#pragma unroll
+        for (int c = 0; c < W; ++c) sacc[(a * W + b) * W + c] += wxy * wz[c];
+      }
+  }
+#pragma unroll
+  for (int o = 0; o < W3; ++o) sh[o * kTileCells + h] = sacc[o];
+  __syncthreads();
+  for (int f = threadIdx.x; f < F3; f += blockDim.x) {
+    const int fx = f / (F * F);
+    const int fy = (f / F) % F;
+    const int fz = f % F;
+    double a = 0.0;
+#pragma unroll
+    for (int ox = 0; ox < W; ++ox) {
+      const int hx = fx - ox;
+      if (hx < 0 || hx >= kTile) continue;
+#pragma unroll
+      for (int oy = 0; oy < W; ++oy) {
+        const int hy = fy - oy;
+        if (hy < 0 || hy >= kTile) continue;
+#pragma unroll
+        for (int oz = 0; oz < W; ++oz) {
+          const int hz = fz - oz;
+          if (hz < 0 || hz >= kTile) continue;
+          a += sh[((ox * W + oy) * W + oz) * kTileCells + (hx * 64 + hy * 8 + hz)];
+        }
+      }
+    }
+    acc[f] = a;
+  }
+  __syncthreads();
+  // Each global cell is written by one footprint cell (its smallest alias
+  // when the footprint wraps onto itself on grids narrower than F).
+  for (int f = threadIdx.x; f < F3; f += blockDim.x) {
+    const int fx = f / (F * F);
+    const int fy = (f / F) % F;
+    const int fz = f % F;
+    if (fx >= g.n[0] || fy >= g.n[1] || fz >= g.n[2]) continue;
+    double v = 0.0;
+    for (int ax = fx; ax < F; ax += g.n[0])
+      for (int ay = fy; ay < F; ay += g.n[1])
+        for (int az = fz; az < F; az += g.n[2]) v += acc[(ax * F + ay) * F + az];
+    if (v == 0.0) continue;
+    int gx = (o0 + fx + OMIN) % g.n[0];
+    int gy = (o1 + fy + OMIN) % g.n[1];
+    int gz = (o2 + fz + OMIN) % g.n[2];
+    if (gx < 0) gx += g.n[0];
+    if (gy < 0) gy += g.n[1];
+    if (gz < 0) gz += g.n[2];
+    grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz] += v;
+  }
+}
+
+template <int S>
+size_t scatter_s_smem() {
+  constexpr int W = Stencil<S>::W;
+  constexpr int F = kTile + W - 1;
+  return sizeof(double) * (W * W * W * kTileCells + F * F * F);
+}
+
 template <int S>
 size_t scatter_smem() {
   constexpr int W = Stencil<S>::W;
@@ -464,6 +591,14 @@ struct Assignor {
     build_colors();
     FC_CUDA(cudaMemsetAsync(totals.get(), 0, totals.bytes(), grid->stream));
     FC_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), grid->stream));
+    for (auto fn : {(const void *)k_scatter_s<0, uint32_t>,
+                    (const void *)k_scatter_s<0, uint64_t>,
+                    (const void *)k_scatter_s<1, uint32_t>,
+                    (const void *)k_scatter_s<1, uint64_t>,
+                    (const void *)k_scatter_s<3, uint32_t>,
+                    (const void *)k_scatter_s<3, uint64_t>})
+      FC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)scatter_s_smem<1>()));
     if (scheme == 2) {
       FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -691,16 +826,16 @@ struct Assignor {
       const uint32_t *ct = tiles + color_offsets[c];
       switch (scheme) {
         case 0:
-          k_scatter<0, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<0>(),
-                               stream()>>>(src_posw, sk, sv,
-                                           tile_start.as<uint32_t>(), ct, geom,
-                                           grid->ptr());
+          k_scatter_s<0, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<0>(),
+                                 stream()>>>(src_posw, sk, sv,
+                                             tile_start.as<uint32_t>(), ct, geom,
+                                             grid->ptr());
           break;
         case 1:
-          k_scatter<1, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<1>(),
-                               stream()>>>(src_posw, sk, sv,
-                                           tile_start.as<uint32_t>(), ct, geom,
-                                           grid->ptr());
+          k_scatter_s<1, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<1>(),
+                                 stream()>>>(src_posw, sk, sv,
+                                             tile_start.as<uint32_t>(), ct, geom,
+                                             grid->ptr());
           break;
         case 2:
           k_scatter<2, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<2>(),
@@ -709,10 +844,10 @@ struct Assignor {
                                            grid->ptr());
           break;
         default:
-          k_scatter<3, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<3>(),
-                               stream()>>>(src_posw, sk, sv,
-                                           tile_start.as<uint32_t>(), ct, geom,
-                                           grid->ptr());
+          k_scatter_s<3, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<3>(),
+                                 stream()>>>(src_posw, sk, sv,
+                                             tile_start.as<uint32_t>(), ct, geom,
+                                             grid->ptr());
           break;
       }
       FC_LAUNCH_CHECK();

@@ -58,6 +58,61 @@ __device__ __forceinline__ float weight_value<float>(const YlmParams &p,
   return ylm_eval_f32(p, D, x, y, z);
 }
 
+// FP32-mixed weighting of one grid row: with (x, y) fixed, Y_lm * r^ell is
+// a polynomial in z, so the row's coefficients (normalisation folded in)
+// are formed once in FP64 and each cell costs a Horner evaluation and one
+// reciprocal:  Y = D * (c0 + c1 z + c2 z^2 + c3 z^3 + c4 z^4) / r^ell.
+struct RowPoly {
+  float c[5];
+  float rxy2;  // x^2 + y^2
+  int ell;
+  float value0;
+};
+
+__device__ __forceinline__ RowPoly row_poly(const YlmParams &p, double x,
+                                            double y) {
+  RowPoly r;
+  r.ell = p.ell;
+  r.value0 = (float)p.value0;
+  const double x2 = x * x, y2 = y * y, s = x2 + y2, n = p.norm;
+  double c[5] = {0, 0, 0, 0, 0};
+  if (p.ell == 2) {
+    switch (p.m) {
+      case 2: c[0] = x2 - y2; break;
+      case 1: c[1] = x; break;
+      case 0: c[0] = -s; c[2] = 2.0; break;
+      case -1: c[1] = y; break;
+      default: c[0] = x * y; break;
+    }
+  } else if (p.ell == 4) {
+    switch (p.m) {
+      case 4: c[0] = x2 * x2 - 6.0 * x2 * y2 + y2 * y2; break;
+      case 3: c[1] = x * (x2 - 3.0 * y2); break;
+      case 2: c[0] = y2 * y2 - x2 * x2; c[2] = 6.0 * (x2 - y2); break;
+      case 1: c[1] = -x * s; c[3] = 4.0 / 3.0 * x; break;
+      case 0: c[0] = 0.375 * s * s; c[2] = -3.0 * s; c[4] = 1.0; break;
+      case -1: c[1] = -y * s; c[3] = 4.0 / 3.0 * y; break;
+      case -2: c[0] = -2.0 * x * y * s; c[2] = 12.0 * x * y; break;
+      case -3: c[1] = 3.0 * x2 * y - y2 * y; break;
+      default: c[0] = 4.0 * x * (x2 * y - y2 * y); break;
+    }
+  }
+  for (int i = 0; i < 5; ++i) r.c[i] = (float)(n * c[i]);
+  r.rxy2 = (float)s;
+  return r;
+}
+
+__device__ __forceinline__ float row_weight(const RowPoly &r, float D,
+                                            double zd) {
+  if (r.ell == 0) return D * r.value0;
+  const float z = (float)zd;
+  const float z2 = z * z;
+  const float poly =
+      (((r.c[4] * z + r.c[3]) * z + r.c[2]) * z + r.c[1]) * z + r.c[0];
+  const float ir2 = 1.0f / (r.rxy2 + z2 + 1e-20f);
+  return r.ell == 2 ? D * poly * ir2 : D * poly * (ir2 * ir2);
+}
+
 // ------------------------------------------------------------------ zfwd
 // B rows of N2 reals per CTA: (optionally Y_lm-weighted) packed as
 // z_j = x_2j + i x_2j+1, length-M complex DFT, then the real-to-complex
@@ -119,19 +174,33 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
 }
 
 // Loads a B-column tile of a strided axis into shared memory.
+// Loads are issued in groups of 8 before any shared-memory store so each
+// thread keeps eight global reads in flight.
 template <int B, typename C>
 __device__ __forceinline__ void load_columns(C *buf, const C *__restrict__ src,
                                              int64_t base, int64_t stride,
                                              int L, int kz0, int h) {
   constexpr int BP = B + 1;
-  for (int idx = threadIdx.x; idx < L * B; idx += blockDim.x) {
-    const int i = idx / B;
-    const int b = idx - i * B;
-    C v;
-    v.x = 0;
-    v.y = 0;
-    if (kz0 + b < h) v = src[base + i * stride + kz0 + b];
-    buf[i * BP + b] = v;
+  const int n = L * B;
+  for (int idx0 = threadIdx.x; idx0 < n; idx0 += 8 * blockDim.x) {
+    C v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = idx0 + u * blockDim.x;
+      const int i = idx / B;
+      const int b = idx - i * B;
+      v[u].x = 0;
+      v[u].y = 0;
+      if (idx < n && kz0 + b < h) v[u] = src[base + i * stride + kz0 + b];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int idx = idx0 + u * blockDim.x;
+      if (idx < n) {
+        const int i = idx / B;
+        buf[i * BP + (idx - i * B)] = v[u];
+      }
+    }
   }
   __syncthreads();
 }
@@ -499,6 +568,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const double cx = x0 + x * 1.0;
   const double cy = y0 + y * 1.0;
   const C *src = reinterpret_cast<const C *>(rho + row * g.n2);
+  RowPoly rp;
+  if constexpr (WEIGHT && sizeof(T) == 4) rp = row_poly(p, cx, cy);
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     v[u].x = 0;
@@ -507,7 +578,10 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
       const int jj = t + Q::TPC * u;
       const C pr = src[jj];
       v[u] = pr;
-      if (WEIGHT) {
+      if constexpr (WEIGHT && sizeof(T) == 4) {
+        v[u].x = row_weight(rp, pr.x, z0 + (2 * jj) * 1.0);
+        v[u].y = row_weight(rp, pr.y, z0 + (2 * jj + 1) * 1.0);
+      } else if constexpr (WEIGHT) {
         v[u].x = weight_value<T>(p, pr.x, cx, cy, z0 + (2 * jj) * 1.0);
         v[u].y = weight_value<T>(p, pr.y, cx, cy, z0 + (2 * jj + 1) * 1.0);
       }

@@ -300,7 +300,8 @@ def test_cross_correlations(fft_path):
     _compare_results(s.results(), sref, FP64_RTOL, "survey-cross")
 
 
-@pytest.mark.parametrize("shape", [(20, 28, 30), (24, 18, 50), (16, 16, 33)])
+@pytest.mark.parametrize("shape", [(20, 28, 30), (24, 18, 50), (16, 16, 33),
+                                   (64, 128, 256), (128, 96, 128)])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_survey_radix_3_5_7_and_odd_sizes(shape, precision):
     """Lengths with factors 3, 5, 7 run through the fused passes; an odd N2
