@@ -282,17 +282,53 @@ def kernel_profile(job, dD, nD, dR, nR):
     return out
 
 
-def algorithmic_bytes(family, w, precision):
-    """Bytes one launch must move at minimum (read + write once)."""
+# DRAM bytes (read + write) per launch of the survey pass kernels at 512^3,
+# FP32-mixed, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
+# of `python bench.py --ngrid 512 --nd 2e6 --nr 1e7 --steps 1 --warmup 1
+# --no-fp64 --no-cpu-baseline`; the pass kernels see the same grid as the
+# full workload (only the catalogs are smaller).  Summaries under profiles/.
+TRAFFIC_PER_LAUNCH_512 = {
+    "zfwd": 1028.45e6,
+}
+
+
+def subgrid_dims(corr):
+    """(r-subgrid edge, k-subgrid shape) of a correlator."""
+    from fftcorr_b200 import _lib
+    rs = (ctypes.c_int * 3)()
+    ks = (ctypes.c_int * 3)()
+    _lib.call("fc_corr_dims", corr.handle, None, None, None, rs, ks)
+    return rs[0], tuple(ks)
+
+
+def algorithmic_bytes(family, w, precision, rs, ks):
+    """HBM bytes one launch must move at minimum (each operand read once,
+    each result written once).  Survey fused passes, N = N0 N1 N2 cells,
+    h = N2/2 + 1, Nc = N0 N1 h complex cells of e bytes (8 FP32, 16 FP64):
+      zfwd   density in (N * s) + W out (Nc * e)
+      yfwd   W in and out (2 Nc e)
+      xcorr  W and G in (2 Nc e) + x-pruned Wr out (rs N1 h e)
+             + k-subgrid read-modify-write (K0 K1 K2 * 16)
+      yinv   Wr in (rs N1 h e) + Wry out (rs rs h e)
+      zinv   Wry in (rs rs h e) + r-subgrid read-modify-write (rs^3 * 16)"""
     s = 8 if precision == "fp64" else 4
-    n = w.ngrid[0] * w.ngrid[1] * w.ngrid[2]
-    nc = w.ngrid[0] * w.ngrid[1] * (w.ngrid[2] // 2 + 1)
+    e = 2 * s
+    n0, n1, n2 = w.ngrid
+    n = n0 * n1 * n2
+    h = n2 // 2 + 1
+    nc = n0 * n1 * h
+    kc = ks[0] * ks[1] * ks[2]
     table = {
-        "weight": n * 8 + n * s,          # rho FP64 in, Y_lm*rho out
+        "zfwd": n * s + nc * e,
+        "yfwd": 2 * nc * e,
+        "xcorr": 2 * nc * e + rs * n1 * h * e + kc * 16,
+        "yinv": rs * n1 * h * e + rs * rs * h * e,
+        "zinv": rs * rs * h * e + rs ** 3 * 16,
+        "weight": n * 8 + n * s,
         "copy_pad": n * 8 + n * s,
-        "conj_mul": 3 * nc * 2 * s,       # F in, G in, F*conj(G) out
-        "r2c": n * s + nc * 2 * s,
-        "c2r": nc * 2 * s + n * s,
+        "conj_mul": 3 * nc * e,
+        "r2c": n * s + nc * e,
+        "c2r": nc * e + n * s,
     }
     return table.get(family)
 
@@ -413,10 +449,12 @@ def main():
         for _ in range(warmup):
             fn()
         dist.barrier()
+        n0 = _lib.launch_count()
         timer.start()
         for _ in range(steps):
             out = fn()
         secs = timer.stop()
+        timed.launches = _lib.launch_count() - n0
         return dist.max(secs), out
 
     # FP32-mixed form: device-resident inputs, then end to end from host.
@@ -424,6 +462,8 @@ def main():
     with ClockSampler(local) as clocks:
         t_dev, (nn, rr, xi) = timed(lambda: job.run_device(dD, nD, dR, nR),
                                     a.steps, a.warmup)
+    launches_dev = timed.launches
+    rs, ks = subgrid_dims(job.corr)
     t_e2e, _ = timed(lambda: job.run_host(D, R), a.steps, 1)
     prof = kernel_profile(job, dD, nD, dR, nR)
     ma_stats = job.maB._stats()
@@ -456,26 +496,29 @@ def main():
     value = world * a.steps / t_dev
     e2e_value = world * a.steps / t_e2e
     peak, peak_kind = measured_hbm_peak()
-    # Roofline of the dominant hand-written kernel (cuFFT's are listed too).
+    # Roofline of the dominant hand-written kernel, and every family's
+    # fraction beside it.
     roof = None
-    ours = {k: v for k, v in prof.items() if k not in ("r2c", "c2r")}
+    fam_roof = {}
+    for fam, v in prof.items():
+        alg = algorithmic_bytes(fam, w, "fp32", rs, ks)
+        if alg and v["launches"]:
+            per = v["seconds"] / v["launches"]
+            fam_roof[fam] = {"achieved_gbs": alg / per / 1e9,
+                             "frac": alg / per / 1e9 / peak,
+                             "us_per_launch": per * 1e6,
+                             "bytes_per_launch": alg}
+    ours = {k: v for k, v in prof.items()
+            if k not in ("r2c", "c2r") and k in fam_roof}
     if ours:
         fam = max(ours, key=lambda k: ours[k]["seconds"])
-        per = ours[fam]["seconds"] / max(1, ours[fam]["launches"])
-        alg = algorithmic_bytes(fam, w, "fp32")
-        if alg:
-            achieved = alg / per / 1e9
-            roof = {"kernel": fam, "bound": "hbm", "achieved": achieved, "peak": peak,
-                    "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                    "bytes_per_launch": alg, "us_per_launch": per * 1e6,
-                    "traffic": None}
-    fft_roof = {}
-    for fam in ("r2c", "c2r"):
-        if fam in prof:
-            per = prof[fam]["seconds"] / max(1, prof[fam]["launches"])
-            alg = algorithmic_bytes(fam, w, "fp32")
-            fft_roof[fam] = {"achieved": alg / per / 1e9, "frac": alg / per / 1e9 / peak,
-                             "us_per_launch": per * 1e6}
+        f = fam_roof[fam]
+        roof = {"kernel": fam, "bound": "hbm", "achieved": f["achieved_gbs"],
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": f["frac"], "bytes_per_launch": f["bytes_per_launch"],
+                "us_per_launch": f["us_per_launch"],
+                "traffic": (TRAFFIC_PER_LAUNCH_512.get(fam)
+                            if tuple(w.ngrid) == (512, 512, 512) else None)}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -485,7 +528,6 @@ def main():
             cpu = {"value": cv, "unit": "jobs/s", "cores": threads,
                    "kind": "reference", "sample": desc}
 
-    gpu_launches = sum(v["launches"] for k, v in prof.items() if k not in ("r2c", "c2r"))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "jobs/s", "n_gpus": world,
@@ -501,13 +543,13 @@ def main():
                     "ms_per_step": 1000.0 * t_e2e / a.steps},
             "fp64_gpu": fp64,
             "roofline": roof,
-            "fft_roofline": fft_roof,
+            "kernel_roofline": fam_roof,
             "kernels": prof,
             "mass_assign_s_per_flush": {"sort": ma_stats.sort_time,
                                         "scatter": ma_stats.window_time},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
-            "gpu_launches": gpu_launches,
+            "gpu_launches": launches_dev,
             "catalog_generation_s": t_gen,
         }
         print(json.dumps(line))

@@ -68,6 +68,7 @@ class KernelTime(ctypes.Structure):
 _SIGNATURES = {
     "fc_last_error": (ctypes.c_char_p, []),
     "fc_version": (ctypes.c_int, []),
+    "fc_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
     "fc_set_device": (ctypes.c_int, [ctypes.c_int]),
     "fc_grid_create": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_double, c_void_pp]),
     "fc_grid_destroy": (ctypes.c_int, [ctypes.c_void_p]),
@@ -187,6 +188,13 @@ def check(rc):
 
 def call(name, *args):
     check(getattr(load(), name)(*args))
+
+
+def launch_count():
+    """This library's own kernel launches issued so far (see fc_api.h)."""
+    n = ctypes.c_ulonglong()
+    call("fc_launch_count", ctypes.byref(n))
+    return n.value
 
 
 def dptr(a):

@@ -563,6 +563,10 @@ struct Assignor {
   uint64_t num_seen = 0;               // particles passed to add calls
   PhaseTimer sort_timer, window_timer;
   double sort_seconds = 0.0, window_seconds = 0.0;
+  // Graph mode (batched form): work goes to stream_override, nothing
+  // synchronises the host, nothing is allocated, phases are not timed.
+  bool graph_mode = false;
+  cudaStream_t stream_override = nullptr;
 
   Assignor(Grid *g, int scheme_, bool periodic_, int64_t buffer_size_)
       : grid(g), scheme(scheme_), periodic(periodic_), buffer_size(buffer_size_) {
@@ -613,7 +617,9 @@ struct Assignor {
     if (grid && grid->stream) cudaStreamSynchronize(grid->stream);
   }
 
-  cudaStream_t stream() const { return grid->stream; }
+  cudaStream_t stream() const {
+    return stream_override ? stream_override : grid->stream;
+  }
 
   void build_colors() {
     int omin = 0;
@@ -807,15 +813,18 @@ struct Assignor {
     size_t temp = 0;
     FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, n, 0,
                                             end_bit, stream()));
+    if (graph_mode)
+      FC_REQUIRE(temp <= cub_temp.bytes(), FC_ERR_STATE,
+                 "sort scratch was not prepared for this many particles");
     cub_temp.resize(temp);
-    sort_timer.start(stream());
+    if (!graph_mode) sort_timer.start(stream());
     FC_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp.get(), temp, dk, dv, n, 0,
                                             end_bit, stream()));
-    sort_timer.stop(stream());
+    if (!graph_mode) sort_timer.stop(stream());
     const KeyT *sk = dk.Current();
     const uint32_t *sv = dv.Current();
     // K-tiles + K-scatter.
-    window_timer.start(stream());
+    if (!graph_mode) window_timer.start(stream());
     k_tile_starts<KeyT><<<grid_for(ntiles + 1, 256), 256, 0, stream()>>>(
         sk, n, ntiles, tile_start.as<uint32_t>());
     FC_LAUNCH_CHECK();
@@ -852,7 +861,7 @@ struct Assignor {
       }
       FC_LAUNCH_CHECK();
     }
-    window_timer.stop(stream());
+    if (!graph_mode) window_timer.stop(stream());
   }
 
   // MassAssignor::flush (mass_assignor.h:127-191).
@@ -863,11 +872,46 @@ struct Assignor {
     else
       flush_typed<uint32_t>();
     count = 0;
+    if (graph_mode) return;
     // Keep the timers' running totals current.
     sort_seconds += sort_timer.seconds();
     sort_timer.clear();
     window_seconds += window_timer.seconds();
     window_timer.clear();
+  }
+
+  // Batched form: size every buffer for up to max_n particles assigned
+  // straight from a device array, so later enqueues allocate nothing.
+  void prepare_graph(int64_t max_n) {
+    graph_mode = true;
+    reserve_keys(std::max<int64_t>(max_n, 1));
+    size_t temp = 0;
+    if (wide_keys) {
+      cub::DoubleBuffer<uint64_t> dk(keys.as<uint64_t>(), keys_alt.as<uint64_t>());
+      cub::DoubleBuffer<uint32_t> dv(vals.as<uint32_t>(), vals_alt.as<uint32_t>());
+      FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, max_n, 0,
+                                              end_bit, stream()));
+    } else {
+      cub::DoubleBuffer<uint32_t> dk(keys.as<uint32_t>(), keys_alt.as<uint32_t>());
+      cub::DoubleBuffer<uint32_t> dv(vals.as<uint32_t>(), vals_alt.as<uint32_t>());
+      FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, max_n, 0,
+                                              end_bit, stream()));
+    }
+    cub_temp.resize(temp + 1024);
+  }
+
+  // Batched form: clear the running totals and assign n particles from a
+  // device array, all enqueued on stream().
+  void enqueue_graph(const double *posw_dev, int64_t n) {
+    FC_CUDA(cudaMemsetAsync(totals.get(), 0, totals.bytes(), stream()));
+    FC_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), stream()));
+    count = 0;
+    num_seen = 0;
+    if (n == 0) return;
+    FC_REQUIRE((size_t)n * key_bytes() <= keys.bytes(), FC_ERR_STATE,
+               "more particles than the batch was prepared for");
+    key_device(posw_dev, n);
+    flush();
   }
 
   void clear() {
@@ -896,6 +940,24 @@ struct Assignor {
     s->window_time = window_seconds;
   }
 };
+
+Assignor *assignor_new(Grid *g, int scheme, bool periodic) {
+  return new Assignor(g, scheme, periodic, 0);
+}
+void assignor_delete(Assignor *a) { delete a; }
+void assignor_prepare_graph(Assignor *a, int64_t max_n, cudaStream_t s) {
+  a->stream_override = s;
+  a->prepare_graph(max_n);
+}
+void assignor_enqueue_graph(Assignor *a, const double *posw, int64_t n,
+                            cudaStream_t s) {
+  a->stream_override = s;
+  a->enqueue_graph(posw, n);
+}
+const double *assignor_totals(const Assignor *a) { return a->totals.as<double>(); }
+const unsigned long long *assignor_counts(const Assignor *a) {
+  return a->counts.as<unsigned long long>();
+}
 
 }  // namespace fc
 

@@ -51,7 +51,14 @@ void set_last_error(const std::string &msg);
     }                                                                     \
   } while (0)
 
-#define FC_LAUNCH_CHECK() FC_CUDA(cudaGetLastError())
+// Host-side count of this library's own kernel launches (every launch site
+// is followed by FC_LAUNCH_CHECK).
+void note_launch();
+#define FC_LAUNCH_CHECK()            \
+  do {                               \
+    ::fc::note_launch();             \
+    FC_CUDA(cudaGetLastError());     \
+  } while (0)
 
 #define FC_REQUIRE(cond, code, msg) \
   do {                              \

@@ -3,6 +3,7 @@
 //
 // ConfigSpaceGrid mirrors cc/grid/config_space_grid.h:10-57 with the grid in
 // HBM; sum/sumsq/add_scalar/multiply_by mirror cc/array/array_ops.cc:55-137.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -19,6 +20,13 @@ thread_local std::string t_last_error;
 void set_last_error(const std::string &msg) { t_last_error = msg; }
 
 const char *last_error_cstr() { return t_last_error.c_str(); }
+
+std::atomic<unsigned long long> &launch_counter() {
+  static std::atomic<unsigned long long> n{0};
+  return n;
+}
+
+void note_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
 
 int sm_count() {
   int dev = 0;
@@ -184,6 +192,13 @@ extern "C" {
 const char *fc_last_error(void) { return fc::last_error_cstr(); }
 
 int fc_version(void) { return 10000 * 0 + 100 * 9 + 0; }
+
+int fc_launch_count(unsigned long long *count) {
+  return guard([&] {
+    FC_REQUIRE(count, FC_ERR_INVALID, "null argument");
+    *count = fc::launch_counter().load(std::memory_order_relaxed);
+  });
+}
 
 int fc_set_device(int device) {
   return guard([&] { FC_CUDA(cudaSetDevice(device)); });

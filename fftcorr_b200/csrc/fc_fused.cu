@@ -102,14 +102,16 @@ __device__ __forceinline__ RowPoly row_poly(const YlmParams &p, double x,
   return r;
 }
 
+// z is the cell's z coordinate rounded to FP32 (the polynomial is FP32).
+// 1/r^2 uses the fast reciprocal-divide intrinsic: r^2 lies between 1e-20
+// and 1e10 here, where its error is 2 ulp, far inside the FP32 budget.
 __device__ __forceinline__ float row_weight(const RowPoly &r, float D,
-                                            double zd) {
+                                            float z) {
   if (r.ell == 0) return D * r.value0;
-  const float z = (float)zd;
   const float z2 = z * z;
   const float poly =
       (((r.c[4] * z + r.c[3]) * z + r.c[2]) * z + r.c[1]) * z + r.c[0];
-  const float ir2 = 1.0f / (r.rxy2 + z2 + 1e-20f);
+  const float ir2 = __fdividef(1.0f, r.rxy2 + z2 + 1e-20f);
   return r.ell == 2 ? D * poly * ir2 : D * poly * (ir2 * ir2);
 }
 
@@ -486,11 +488,22 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const int64_t base = (int64_t)yy * g.h + kzi;
   auto exf = [&](int i) { return &ex[i * Q::BP + b]; };
   C v[8];
+  // In product mode the G column is loaded together with the W column, so
+  // both streams are in flight during the forward transform.
+  C gv[MODE == 0 ? 1 : 8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     v[u].x = 0;
     v[u].y = 0;
     if (valid) v[u] = W[base + (t + Q::TPC * u) * stride];
+  }
+  if constexpr (MODE != 0) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      gv[u].x = 0;
+      gv[u].y = 0;
+      if (valid) gv[u] = G[base + (t + Q::TPC * u) * stride];
+    }
   }
   reg_fft<L>(v, t, exf, tabx, -1);
   if constexpr (MODE == 0) {
@@ -500,8 +513,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
     }
   } else {
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (valid) v[u] = cmulc(v[u], G[base + (t + Q::TPC * u) * stride]);
+    for (int u = 0; u < 8; ++u) v[u] = cmulc(v[u], gv[u]);
     // k-subgrid extraction (see k_xcorr): needs P at arbitrary rows.
     const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
     if (ksub != nullptr && kz0 <= oz) {
@@ -569,7 +581,13 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const double cy = y0 + y * 1.0;
   const C *src = reinterpret_cast<const C *>(rho + row * g.n2);
   RowPoly rp;
-  if constexpr (WEIGHT && sizeof(T) == 4) rp = row_poly(p, cx, cy);
+  // z of this thread's first element in FP64; the elements u step by the
+  // exact integer 2 TPC, added in FP32.
+  float zt = 0.f;
+  if constexpr (WEIGHT && sizeof(T) == 4) {
+    rp = row_poly(p, cx, cy);
+    zt = (float)(z0 + (2 * t) * 1.0);
+  }
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     v[u].x = 0;
@@ -579,8 +597,9 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
       const C pr = src[jj];
       v[u] = pr;
       if constexpr (WEIGHT && sizeof(T) == 4) {
-        v[u].x = row_weight(rp, pr.x, z0 + (2 * jj) * 1.0);
-        v[u].y = row_weight(rp, pr.y, z0 + (2 * jj + 1) * 1.0);
+        const float zu = zt + (float)(2 * Q::TPC * u);
+        v[u].x = row_weight(rp, pr.x, zu);
+        v[u].y = row_weight(rp, pr.y, zu + 1.0f);
       } else if constexpr (WEIGHT) {
         v[u].x = weight_value<T>(p, pr.x, cx, cy, z0 + (2 * jj) * 1.0);
         v[u].y = weight_value<T>(p, pr.y, cx, cy, z0 + (2 * jj + 1) * 1.0);

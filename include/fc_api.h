@@ -248,6 +248,11 @@ int fc_sum_sumsq_static(const double *device_data, int64_t n, double *sum,
                         double *sumsq);
 
 /* ------------------------------------------------------------- utilities */
+/* Number of this library's own kernel launches issued so far by the host, in
+ * all threads (cuFFT's and CUB's kernels are not included; a replayed CUDA
+ * graph counts its kernels when it is captured, not when it is replayed).
+ * Has no counterpart in the reference. */
+int fc_launch_count(unsigned long long *count);
 /* Waits for all work on the current device. */
 int fc_device_synchronize(void);
 /* Page-locks an existing host range so copies from it run at full PCIe
