@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--maxell", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-boxes", type=int, default=64)
+    ap.add_argument("--only-batched", action="store_true")
     return ap.parse_args()
 
 
@@ -333,6 +336,64 @@ def algorithmic_bytes(family, w, precision, rs, ks):
     return table.get(family)
 
 
+# --------------------------------------------------------- batched form
+
+def batched_boxes(nboxes, seed0=4):
+    """64 periodic mock boxes: L ~ U[1000, 2000] Mpc/h, N from
+    {128, 192, 256, 384}^3, Np log-uniform in [0.5M, 8M], clustered (1e4
+    centres, sigma 5 Mpc/h), seed 4 + i; catalogs generated on the device."""
+    from fftcorr_b200 import catalog
+    boxes, desc = [], []
+    for i in range(nboxes):
+        rng = np.random.default_rng(seed0 + i)
+        L = float(rng.uniform(1000.0, 2000.0))
+        n = int(rng.choice([128, 192, 256, 384]))
+        npart = int(np.exp(rng.uniform(np.log(0.5e6), np.log(8e6))))
+        cat = catalog.clustered_box(npart, L, seed=seed0 + i, ncentres=10000,
+                                    sigma=5.0)
+        boxes.append(((n, n, n), L / n, cat))
+        desc.append((n, npart))
+    return boxes, desc
+
+
+def run_batched(a, timed_fn):
+    from fftcorr_b200 import _lib
+    from fftcorr_b200.batch import PeriodicBatch
+    from fftcorr_b200.correlate import NO_CORRECTION
+    from fftcorr_b200.particle_mesh import DistributionScheme
+    boxes, desc = batched_boxes(a.batch_boxes)
+    out = {}
+    for prec in ("fp32", "fp64"):
+        if prec == "fp64" and a.no_fp64:
+            continue
+        t0 = time.perf_counter()
+        b = PeriodicBatch(boxes, DistributionScheme.CLOUD_IN_CELL, rmax=200.0,
+                          dr=5.0, kmax=0.1, dk=0.005, maxell=2,
+                          window_correct=NO_CORRECTION, precision=prec)
+        build_s = time.perf_counter() - t0
+        for _ in range(max(3, a.warmup)):
+            b.run()
+        n0 = _lib.launch_count()
+        secs = [b.run() for _ in range(a.steps)]
+        info = b.info
+        t = float(np.sum(secs))
+        out[prec] = {
+            "value": len(boxes) * a.steps / t, "unit": "boxes/s",
+            "ms_per_batch": 1000.0 * t / a.steps,
+            "ms_per_batch_min": 1000.0 * min(secs),
+            "build_and_tune_s": build_s, "info": info,
+            "host_launches_per_replay": (_lib.launch_count() - n0) // max(1, a.steps),
+        }
+        del b
+    npart = sum(d[1] for d in desc)
+    cells = sum(d[0] ** 3 for d in desc)
+    return {"workload": f"{len(boxes)} periodic boxes, L U[1000,2000], N in "
+                        "{128,192,256,384}^3, Np log-uniform [0.5M, 8M] clustered "
+                        "(1e4 centres, sigma 5), CIC, ell<=2, rmax 200 dr 5, "
+                        "kmax 0.1 dk 0.005; one CUDA graph per replay",
+            "particles": npart, "cells": cells, "forms": out}
+
+
 # --------------------------------------------------------- CPU baseline
 
 def cpu_baseline_sample(w, R, threads):
@@ -435,6 +496,11 @@ def main():
     from fftcorr_b200 import _lib
     _lib.call("fc_set_device", local)
     dist = Dist(world)
+    if a.only_batched:
+        if rank == 0:
+            print(json.dumps({"batched": run_batched(a, None)}))
+        dist.close()
+        return
     w = Workload(a)
     t_gen = time.perf_counter()
     D, R = w.catalogs(seed_offset=rank)
@@ -520,6 +586,8 @@ def main():
                 "traffic": (TRAFFIC_PER_LAUNCH_512.get(fam)
                             if tuple(w.ngrid) == (512, 512, 512) else None)}
 
+    batched = None if a.no_batched else run_batched(a, None)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -551,6 +619,7 @@ def main():
             "cpu_baseline": cpu,
             "gpu_launches": launches_dev,
             "catalog_generation_s": t_gen,
+            "batched": batched,
         }
         print(json.dumps(line))
     for p in (dD, dR):

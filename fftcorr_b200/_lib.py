@@ -64,6 +64,26 @@ class KernelTime(ctypes.Structure):
                 ("seconds", ctypes.c_double)]
 
 
+class BatchBox(ctypes.Structure):
+    _fields_ = [("shape", ctypes.c_int * 3), ("cell_size", ctypes.c_double),
+                ("posw_device", ctypes.c_void_p), ("n", ctypes.c_int64)]
+
+
+class BatchParams(ctypes.Structure):
+    _fields_ = [("scheme", ctypes.c_int), ("window", ctypes.c_int),
+                ("rmax", ctypes.c_double), ("dr", ctypes.c_double),
+                ("kmax", ctypes.c_double), ("dk", ctypes.c_double),
+                ("maxell", ctypes.c_int), ("precision", ctypes.c_int),
+                ("lanes", ctypes.c_int), ("tune", ctypes.c_int)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("nboxes", ctypes.c_int), ("lanes", ctypes.c_int),
+                ("hist_blocks", ctypes.c_int), ("graph_nodes", ctypes.c_int64),
+                ("kernel_nodes", ctypes.c_int64), ("own_kernel_nodes", ctypes.c_int64),
+                ("hist_items", ctypes.c_int64), ("device_bytes", ctypes.c_int64)]
+
+
 # name -> (restype, argtypes); every fc_* entry returns an fc_status int.
 _SIGNATURES = {
     "fc_last_error": (ctypes.c_char_p, []),
@@ -92,6 +112,9 @@ _SIGNATURES = {
                                                   ctypes.c_double, ctypes.c_int64]),
     "fc_assignor_add_posw_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p,
                                                    ctypes.c_int64]),
+    "fc_assignor_add_random": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64,
+                                              ctypes.c_double, c_double_p,
+                                              ctypes.c_uint64, ctypes.c_int64]),
     "fc_assignor_flush": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_assignor_clear": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_assignor_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AssignStats)]),
@@ -131,10 +154,43 @@ _SIGNATURES = {
     "fc_device_malloc": (ctypes.c_int, [ctypes.c_size_t, c_void_pp]),
     "fc_device_free": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_memcpy_htod": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "fc_memcpy_dtoh": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "fc_timer_create": (ctypes.c_int, [c_void_pp]),
     "fc_timer_start": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_timer_stop": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
     "fc_timer_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fc_catalog_uniform": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_double_p,
+                                          c_double_p, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_uint64]),
+    "fc_catalog_clustered_box": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64,
+                                                ctypes.c_double, ctypes.c_int,
+                                                ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, ctypes.c_uint64]),
+    "fc_catalog_sector": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_uint64]),
+    "fc_apply_displacement": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_int64,
+                                             c_double_p, ctypes.c_int, c_double_p]),
+    "fc_batch_params_default": (ctypes.c_int, [ctypes.POINTER(BatchParams)]),
+    "fc_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchBox), ctypes.c_int,
+                                       ctypes.POINTER(BatchParams), c_void_pp]),
+    "fc_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fc_batch_run": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "fc_batch_launch": (ctypes.c_int, [ctypes.c_void_p]),
+    "fc_batch_wait": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),
+    "fc_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(BatchInfo)]),
+    "fc_batch_box_dims": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_int_p, c_int_p,
+                                         c_int_p]),
+    "fc_batch_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_double_p,
+                                        c_int_p, c_double_p, c_double_p, c_int_p,
+                                        c_double_p, c_double_p]),
+    "fc_batch_box_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.POINTER(AssignStats)]),
+    "fc_tune_export": (ctypes.c_int, [ctypes.c_char_p]),
+    "fc_tune_import": (ctypes.c_int, [ctypes.c_char_p]),
+    "fc_tune_forget": (ctypes.c_int, []),
+    "fc_tune_count": (ctypes.c_int, [c_int_p]),
     "fc_hist_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, c_void_pp]),
     "fc_hist_destroy": (ctypes.c_int, [ctypes.c_void_p]),

@@ -914,6 +914,52 @@ struct Assignor {
     flush();
   }
 
+  // add_random_particles (fftcorr/catalog/random_catalog.py:8-87) with the
+  // positions drawn on the device: uniform over the grid's box, optionally
+  // displaced by a gridded field, weight w each, in batches of `batch`.
+  void add_random(int64_t n, double w, const double *disp_host, uint64_t seed,
+                  int64_t batch) {
+    FC_REQUIRE(n >= 0, FC_ERR_INVALID, "negative particle count");
+    if (n == 0) return;
+    if (batch <= 0) batch = (int64_t)1 << 26;
+    const int64_t nb_max = std::min(batch, n);
+    DeviceBuffer gen((size_t)nb_max * 4 * sizeof(double));
+    DeviceBuffer ddisp, dflag(sizeof(int));
+    AssignGeomLite lite;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lite.n[a] = geom.n[a];
+      lite.posmin[a] = geom.posmin[a];
+      lo[a] = geom.posmin[a];
+      hi[a] = geom.posmin[a] + geom.n[a] * geom.cell;
+    }
+    lite.cell = geom.cell;
+    lite.periodic = geom.periodic;
+    FC_CUDA(cudaMemsetAsync(dflag.get(), 0, sizeof(int), stream()));
+    if (disp_host) {
+      const size_t nd = (size_t)geom.n[0] * geom.n[1] * geom.n[2] * 3;
+      ddisp.resize(nd * sizeof(double));
+      FC_CUDA(cudaMemcpyAsync(ddisp.get(), disp_host, nd * sizeof(double),
+                              cudaMemcpyHostToDevice, stream()));
+    }
+    for (int64_t done = 0; done < n;) {
+      const int64_t nb = std::min(nb_max, n - done);
+      catalog_uniform(gen.as<double>(), done, nb, lo, hi, w, w, seed, stream());
+      if (disp_host)
+        displace(gen.as<double>(), 4, nb, ddisp.as<double>(), lite,
+                 gen.as<double>(), 4, dflag.as<int>(), stream());
+      add_device_posw(gen.as<double>(), nb, cudaMemcpyDeviceToDevice);
+      done += nb;
+    }
+    int flag = 0;
+    FC_CUDA(cudaMemcpyAsync(&flag, dflag.get(), sizeof(int),
+                            cudaMemcpyDeviceToHost, stream()));
+    FC_CUDA(cudaStreamSynchronize(stream()));
+    FC_REQUIRE(!flag, FC_ERR_INVALID,
+               "Failed to apply displacement field: coordinates out of bounds? "
+               "Try setting periodic_wrap=True.");
+  }
+
   void clear() {
     FC_CUDA(cudaStreamSynchronize(stream()));
     count = 0;
@@ -1004,6 +1050,13 @@ int fc_assignor_add_posw_device(fc_assignor *ma, const double *posw_device,
     FC_REQUIRE(posw_device || n == 0, FC_ERR_INVALID, "null particle array");
     a->add_device_posw(posw_device, n, cudaMemcpyDeviceToDevice);
     FC_CUDA(cudaStreamSynchronize(a->stream()));
+  });
+}
+
+int fc_assignor_add_random(fc_assignor *ma, int64_t n, double particle_weight,
+                           const double *disp, uint64_t seed, int64_t batch_size) {
+  return guard([&] {
+    as_assignor(ma)->add_random(n, particle_weight, disp, seed, batch_size);
   });
 }
 

@@ -183,6 +183,14 @@ inline unsigned grid_for(size_t n, int block, int waves = 8) {
   return (unsigned)blocks;
 }
 
+// Launch shape of a grid-stride kernel: threads per block and at most
+// `waves` blocks per SM.
+struct LaunchShape {
+  int threads;
+  int waves;
+  unsigned grid(size_t n) const { return grid_for(n, threads, waves); }
+};
+
 // ------------------------------------------------------------ reductions
 
 // Deterministic block sum: fixed shuffle tree inside each warp, then warp

@@ -449,6 +449,12 @@ int fc_memcpy_htod(void *dst, const void *src, size_t bytes) {
   });
 }
 
+int fc_memcpy_dtoh(void *dst, const void *src, size_t bytes) {
+  return guard([&] {
+    FC_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
 int fc_timer_create(fc_timer **t) {
   return guard([&] {
     FC_REQUIRE(t, FC_ERR_INVALID, "null pointer");

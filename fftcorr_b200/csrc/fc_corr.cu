@@ -404,6 +404,14 @@ struct Correlator {
   cudaEvent_t ev_fft0 = nullptr, ev_fft1 = nullptr;
   double last_total = 0.0;
   int n_fft = 0;
+  // Launch shapes of the grid-stride kernels; results do not depend on them
+  // (every cell is computed independently), so the autotuner may change them.
+  LaunchShape ls_abs2{256, 8}, ls_ksub{256, 8}, ls_rsub{256, 8};
+  // Deferred-histogram mode (batched form): each multipole keeps its own
+  // subgrids and the histograms are reduced later, for many correlators at
+  // once.
+  bool deferred = false;
+  std::vector<DeviceBuffer> rsub_l, ksub_l;
 
   Correlator(int kind_, const int shape[3], double cell, const double pmin[3],
              int window, double rmax, double dr, double kmax, double dk,
@@ -610,7 +618,8 @@ struct Correlator {
     const size_t nc = geo.ncomplex();
     // The work grid has padded rows of n2p/2 complex = ncomplex overall.
     if (autocorr) {
-      k_abs2<C><<<grid_for(nc, 256), 256, 0, stream>>>(work.as<C>(), nc);
+      k_abs2<C><<<ls_abs2.grid(nc), ls_abs2.threads, 0, stream>>>(work.as<C>(),
+                                                                   nc);
     } else {
       k_conj_mul<C><<<grid_for(nc, 256), 256, 0, stream>>>(work.as<C>(),
                                                            g2.as<C>(), nc);
@@ -619,24 +628,24 @@ struct Correlator {
   }
 
   template <typename T>
-  void ksub_acc(int ell, int m, double coeff) {
+  void ksub_acc(int ell, int m, double coeff, double *dst = nullptr) {
     Profiler::Scope ps(&prof, stream, "ksub");
     using C = typename Cplx<T>::type;
     const double *ax = d_kaxes.as<double>();
     const double *wn = d_kwin.as<double>();
     const int a = geo.kshape[0], b = geo.kshape[1];
-    k_ksub<C><<<grid_for(geo.kcells(), 256), 256, 0, stream>>>(
-        work.as<C>(), ksub.as<double>(), geo.kshape[0], geo.kshape[1],
+    k_ksub<C><<<ls_ksub.grid(geo.kcells()), ls_ksub.threads, 0, stream>>>(
+        work.as<C>(), dst ? dst : ksub.as<double>(), geo.kshape[0], geo.kshape[1],
         geo.kshape[2], geo.shape[0], geo.shape[1], geo.n2p() / 2, ax, ax + a,
         ax + a + b, wn, wn + a, wn + a + b, make_ylm_params(ell, m, coeff));
     FC_LAUNCH_CHECK();
   }
 
   template <typename T>
-  void rsub_acc(int ell, int m, double coeff) {
+  void rsub_acc(int ell, int m, double coeff, double *dst = nullptr) {
     Profiler::Scope ps(&prof, stream, "rsub");
-    k_rsub<T><<<grid_for(geo.rcells(), 256), 256, 0, stream>>>(
-        work.as<T>(), rsub.as<double>(), geo.rsize, geo.shape[0], geo.shape[1],
+    k_rsub<T><<<ls_rsub.grid(geo.rcells()), ls_rsub.threads, 0, stream>>>(
+        work.as<T>(), dst ? dst : rsub.as<double>(), geo.rsize, geo.shape[0], geo.shape[1],
         geo.shape[2], geo.n2p(), d_raxis.as<double>(),
         make_ylm_params(ell, m, coeff));
     FC_LAUNCH_CHECK();
@@ -748,6 +757,62 @@ struct Correlator {
       rsub_acc<T>(ell, 0, coeff);
       hist_rows(ell, true, false);
       if (ell == 0) save_zerolag();
+    }
+  }
+
+  // Deferred-histogram mode: one r- and one k-subgrid per multipole.
+  void make_deferred() {
+    FC_REQUIRE(kind == FC_PERIODIC && !fused, FC_ERR_UNSUPPORTED,
+               "deferred histograms are built for the periodic correlator");
+    deferred = true;
+    rsub_l.resize(geo.nrows);
+    ksub_l.resize(geo.nrows);
+    for (int r = 0; r < geo.nrows; ++r) {
+      rsub_l[r].resize(geo.rcells() * sizeof(double));
+      ksub_l[r].resize(geo.kcells() * sizeof(double));
+    }
+  }
+
+  // PeriodicCorrelator::correlate_internal (correlator.h:273-357) on a
+  // density the caller has already written into the padded work grid, with
+  // the histograms deferred (hist_work).  Enqueue only: no allocation, no
+  // host synchronisation, so it can be captured into a CUDA graph.
+  template <typename T>
+  void periodic_prepared() {
+    const size_t ncells = geo.ncells();
+    exec_r2c(work.get(), work.get());
+    conj_mul<T>(true);
+    const double k_rescale = geo.cell * geo.cell * geo.cell / (double)ncells;
+    const int maxell = 2 * (geo.nrows - 1);
+    for (int ell = 0; ell <= maxell; ell += 2) {
+      double *dst = ksub_l[ell / 2].as<double>();
+      FC_CUDA(cudaMemsetAsync(dst, 0, geo.kcells() * sizeof(double), stream));
+      const double coeff = sqrt((4.0 * M_PI) * (2 * ell + 1)) * k_rescale;
+      ksub_acc<T>(ell, 0, coeff, dst);
+    }
+    exec_c2r(work.get(), work.get());
+    const double r_rescale = (1.0 / ncells / ncells);
+    for (int ell = 0; ell <= maxell; ell += 2) {
+      double *dst = rsub_l[ell / 2].as<double>();
+      FC_CUDA(cudaMemsetAsync(dst, 0, geo.rcells() * sizeof(double), stream));
+      const double coeff = sqrt((4.0 * M_PI) * (2 * ell + 1)) * r_rescale;
+      rsub_acc<T>(ell, 0, coeff, dst);
+    }
+    const size_t rz = ((size_t)geo.rmax_cells * geo.rsize + geo.rmax_cells) *
+                          geo.rsize + geo.rmax_cells;
+    FC_CUDA(cudaMemcpyAsync(d_zerolag.get(), rsub_l[0].as<double>() + rz,
+                            sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    have_result = true;
+  }
+
+  // The histogram reductions of the deferred subgrids as work items.
+  void hist_work(std::vector<HistItem> &items, std::vector<FoldItem> &folds) {
+    FC_REQUIRE(deferred, FC_ERR_STATE, "correlator is not in deferred mode");
+    for (int r = 0; r < geo.nrows; ++r) {
+      rbins.append_work(rsub_l[r].as<double>(), d_rhist.as<double>() + r * geo.nr,
+                        items, folds);
+      kbins.append_work(ksub_l[r].as<double>(), d_khist.as<double>() + r * geo.nk,
+                        items, folds);
     }
   }
 
@@ -865,6 +930,63 @@ struct Correlator {
                          cudaMemcpyDeviceToHost));
   }
 };
+
+Correlator *correlator_new(int kind, const int shape[3], double cell,
+                           const double posmin[3], int window, double rmax,
+                           double dr, double kmax, double dk, int maxell,
+                           int precision) {
+  Correlator *c = new Correlator(kind, shape, cell, posmin, window, rmax, dr,
+                                 kmax, dk, maxell, precision);
+  try {
+    FC_CUDA(cudaStreamSynchronize(c->stream));
+  } catch (...) {
+    delete c;
+    throw;
+  }
+  return c;
+}
+void correlator_delete(Correlator *c) { delete c; }
+void correlator_make_deferred(Correlator *c) { c->make_deferred(); }
+void *correlator_work(Correlator *c) { return c->work.get(); }
+void correlator_set_stream(Correlator *c, cudaStream_t s) { c->set_stream(s); }
+void correlator_enqueue_prepared(Correlator *c) {
+  if (c->fp64())
+    c->periodic_prepared<double>();
+  else
+    c->periodic_prepared<float>();
+}
+void correlator_hist_work(Correlator *c, std::vector<HistItem> &items,
+                          std::vector<FoldItem> &folds) {
+  c->hist_work(items, folds);
+}
+void correlator_results(Correlator *c, double *rbins, int *rcounts,
+                        double *rhist, double *kbins, int *kcounts,
+                        double *khist, double *zerolag) {
+  c->results(rbins, rcounts, rhist, kbins, kcounts, khist, zerolag);
+}
+void correlator_dims(const Correlator *c, int *nrows, int *nr, int *nk) {
+  if (nrows) *nrows = c->geo.nrows;
+  if (nr) *nr = c->geo.nr;
+  if (nk) *nk = c->geo.nk;
+}
+CorrShapes correlator_shapes(Correlator *c) {
+  return CorrShapes{&c->ls_abs2, &c->ls_ksub, &c->ls_rsub};
+}
+void correlator_time_kernels(Correlator *c, int which, cudaStream_t s) {
+  c->set_stream(s);
+  const int ell = c->geo.nrows > 1 ? 2 : 0;
+  double *k = c->deferred ? c->ksub_l[0].as<double>() : c->ksub.as<double>();
+  double *r = c->deferred ? c->rsub_l[0].as<double>() : c->rsub.as<double>();
+  if (c->fp64()) {
+    if (which == 0) c->conj_mul<double>(true);
+    if (which == 1) c->ksub_acc<double>(ell, 0, 1.0, k);
+    if (which == 2) c->rsub_acc<double>(ell, 0, 1.0, r);
+  } else {
+    if (which == 0) c->conj_mul<float>(true);
+    if (which == 1) c->ksub_acc<float>(ell, 0, 1.0, k);
+    if (which == 2) c->rsub_acc<float>(ell, 0, 1.0, r);
+  }
+}
 
 // Device bytes of a correlator (see Correlator::allocate and make_plans);
 // the cuFFT work area is estimated as one complex grid.

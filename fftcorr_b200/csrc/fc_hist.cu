@@ -124,6 +124,9 @@ void BinIndex::build(int *bins_dev, int64_t n, int nbins_, cudaStream_t s) {
   }
   cf[nbins] = (int)cs.size();
   nchunks = (int)cs.size();
+  h_chunk_start = cs;
+  h_chunk_len = cl;
+  h_chunk_first = cf;
   perm.resize(std::max<int64_t>(ninrange, 1) * sizeof(uint32_t));
   if (ninrange > 0)
     FC_CUDA(cudaMemcpyAsync(perm.get(), dv.Current(),
@@ -148,7 +151,7 @@ void BinIndex::build(int *bins_dev, int64_t n, int nbins_, cudaStream_t s) {
 void BinIndex::reduce(const double *values, double *hist_row,
                       cudaStream_t s) const {
   if (nchunks > 0) {
-    k_chunk_sums<<<nchunks, 256, 0, s>>>(values, perm.as<uint32_t>(),
+    k_chunk_sums<<<nchunks, kHistThreads, 0, s>>>(values, perm.as<uint32_t>(),
                                          chunk_start.as<uint32_t>(),
                                          chunk_len.as<int>(),
                                          partials.as<double>());
@@ -164,7 +167,7 @@ void BinIndex::reduce(const double *values, double *hist_row,
 void BinIndex::reduce_add(const double *values, double *hist_row,
                           cudaStream_t s) const {
   if (nchunks > 0) {
-    k_chunk_sums<<<nchunks, 256, 0, s>>>(values, perm.as<uint32_t>(),
+    k_chunk_sums<<<nchunks, kHistThreads, 0, s>>>(values, perm.as<uint32_t>(),
                                          chunk_start.as<uint32_t>(),
                                          chunk_len.as<int>(),
                                          partials.as<double>());
@@ -175,6 +178,19 @@ void BinIndex::reduce_add(const double *values, double *hist_row,
         partials.as<double>(), chunk_first.as<int>(), nbins, hist_row, 1);
     FC_LAUNCH_CHECK();
   }
+}
+
+void BinIndex::append_work(const double *values, double *hist_row,
+                           std::vector<HistItem> &items,
+                           std::vector<FoldItem> &folds) const {
+  const int base = (int)items.size();
+  for (int c = 0; c < nchunks; ++c)
+    items.push_back(HistItem{values, perm.as<uint32_t>(), h_chunk_start[c],
+                             h_chunk_len[c]});
+  for (int b = 0; b < nbins; ++b)
+    folds.push_back(FoldItem{base + h_chunk_first[b],
+                             h_chunk_first[b + 1] - h_chunk_first[b],
+                             hist_row + b});
 }
 
 // HistogramList with its counts and sums in device memory.

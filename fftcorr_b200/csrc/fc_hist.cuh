@@ -19,6 +19,23 @@ namespace fc {
 
 // Values per histogram chunk (one CTA each).
 constexpr int kHistChunk = 2048;
+// Threads of a chunk reduction: part of the summation order, so fixed.
+constexpr int kHistThreads = 256;
+
+// One chunk of a histogram reduction: the sum of values[perm[start ..
+// start + len)] (k_chunk_sums' fixed tree) goes to partials[item index].
+struct HistItem {
+  const double *values;
+  const uint32_t *perm;
+  uint32_t start;
+  int len;
+};
+// One bin: *dest = sum of partials[first .. first + count) in order.
+struct FoldItem {
+  int first;
+  int count;
+  double *dest;
+};
 
 struct BinIndex {
   int nbins = 0;
@@ -31,6 +48,8 @@ struct BinIndex {
   DeviceBuffer chunk_len;           // int per chunk
   DeviceBuffer chunk_first;         // int per bin + 1: first chunk of bin
   DeviceBuffer partials;            // double per chunk
+  std::vector<uint32_t> h_chunk_start;  // host copies of the chunk table
+  std::vector<int> h_chunk_len, h_chunk_first;
 
   // Builds the index from device bin ids (values outside [0, nbins) are
   // excluded).  bins_dev is clobbered.  Synchronises the stream.
@@ -41,6 +60,11 @@ struct BinIndex {
   // hist_row[b] += that sum.
   void reduce_add(const double *values, double *hist_row,
                   cudaStream_t s) const;
+  // Appends the work of reduce(values, hist_row) as chunk and fold items
+  // (the same sums in the same order).
+  void append_work(const double *values, double *hist_row,
+                   std::vector<HistItem> &items,
+                   std::vector<FoldItem> &folds) const;
 };
 
 // Bin index of value v for HistogramList(minval, binsize, nbins); -1 when

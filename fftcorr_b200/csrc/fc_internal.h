@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "fc_common.cuh"
+#include "fc_hist.cuh"
 
 namespace fc {
 
@@ -75,6 +76,25 @@ inline void stream_after(cudaStream_t waiter, cudaStream_t producer) {
   cudaEventDestroy(ev);
 }
 
+// ------------------------------------------------------ device catalogs
+// Grid geometry for the displacement kernel.
+struct AssignGeomLite {
+  int n[3];
+  double posmin[3];
+  double cell;
+  int periodic;
+};
+// Particles first .. first+n of the counter-based uniform catalog (seed) into
+// posw[0 .. n): positions uniform in [lo, hi), weights w0 + (w1 - w0) u.
+void catalog_uniform(double *posw, int64_t first, int64_t n, const double lo[3],
+                     const double hi[3], double w0, double w1, uint64_t seed,
+                     cudaStream_t s);
+// out[i] = pos[i] + disp[cell of pos[i]]; *flag = 1 if some position has no
+// cell.  Rows of pos and out are `stride` / `out_stride` doubles apart.
+void displace(const double *pos, int stride, int64_t n, const double *disp,
+              const AssignGeomLite &g, double *out, int out_stride, int *flag,
+              cudaStream_t s);
+
 // ----------------------------------------------- batched-form building blocks
 // Enqueue-only entry points used by the batched form (fc_batch.cu): once
 // prepared they allocate nothing and never synchronise the host, so a whole
@@ -88,36 +108,35 @@ void assignor_enqueue_graph(Assignor *a, const double *posw, int64_t n,
 const double *assignor_totals(const Assignor *a);  // device [totw, totwsq]
 const unsigned long long *assignor_counts(const Assignor *a);  // [num_added]
 
-// One chunk of a deterministic histogram reduction (see fc_hist.cuh): the
-// sum of values[perm[start .. start+len)] goes to partials[index].
-struct HistItem {
-  const double *values;
-  const uint32_t *perm;
-  uint32_t start;
-  int len;
-};
-// One bin: dest = sum of partials[first .. first+count) in order.
-struct FoldItem {
-  int first;
-  int count;
-  double *dest;
-};
-
 struct Correlator;
-Correlator *correlator_new_periodic(const int shape[3], double cell, int window,
-                                    double rmax, double dr, double kmax,
-                                    double dk, int maxell, int precision);
+Correlator *correlator_new(int kind, const int shape[3], double cell,
+                           const double posmin[3], int window, double rmax,
+                           double dr, double kmax, double dk, int maxell,
+                           int precision);
 void correlator_delete(Correlator *c);
-// Enqueues a periodic autocorrelation of rho on s with the histograms
-// deferred (every multipole keeps its own subgrids).
-void correlator_enqueue_deferred(Correlator *c, const double *rho,
-                                 cudaStream_t s);
-// Appends the histogram work of the last deferred run.
+// Periodic correlators only: every multipole keeps its own subgrids and the
+// histograms are left to the caller (correlator_hist_work).
+void correlator_make_deferred(Correlator *c);
+// The padded real work grid [N0][N1][2(N2/2+1)] in the correlator's
+// precision.
+void *correlator_work(Correlator *c);
+void correlator_set_stream(Correlator *c, cudaStream_t s);
+// Enqueues a periodic autocorrelation of the density already in the work
+// grid (deferred mode; no allocation or host synchronisation).
+void correlator_enqueue_prepared(Correlator *c);
+// Appends the histogram reductions of the last deferred run.
 void correlator_hist_work(Correlator *c, std::vector<HistItem> &items,
                           std::vector<FoldItem> &folds);
 void correlator_results(Correlator *c, double *rbins, int *rcounts,
                         double *rhist, double *kbins, int *kcounts,
                         double *khist, double *zerolag);
 void correlator_dims(const Correlator *c, int *nrows, int *nr, int *nk);
+struct CorrShapes {
+  LaunchShape *abs2, *ksub, *rsub;
+};
+CorrShapes correlator_shapes(Correlator *c);
+// Launches one of the tunable kernels (0 |F|^2, 1 k-subgrid, 2 r-subgrid)
+// on s, for timing.
+void correlator_time_kernels(Correlator *c, int which, cudaStream_t s);
 
 }  // namespace fc

@@ -133,6 +133,17 @@ int fc_assignor_add_pos_weight(fc_assignor *ma, const double *pos,
 int fc_assignor_add_posw_device(fc_assignor *ma, const double *posw_device,
                                 int64_t n);
 /* MassAssignor::flush (mass_assignor.h:127-191). */
+/* add_random_particles (fftcorr/catalog/random_catalog.py:8-87) with the
+ * positions generated on the device: n points uniform over the grid's box
+ * [posmin, posmin + shape * cell), each of weight particle_weight, displaced
+ * by disp (host (N0, N1, N2, 3) FP64 field, as apply_displacement_field;
+ * NULL for none), assigned in batches of batch_size (<= 0: 2^26).  The
+ * generator is Philox4x32-10 keyed by seed, so the catalog does not depend
+ * on batch_size; it differs value by value from numpy's generator.  Fails
+ * with FC_ERR_INVALID if a displaced point leaves a non-periodic grid. */
+int fc_assignor_add_random(fc_assignor *ma, int64_t n, double particle_weight,
+                           const double *disp, uint64_t seed,
+                           int64_t batch_size);
 int fc_assignor_flush(fc_assignor *ma);
 /* MassAssignor::clear (mass_assignor.h:60-70). */
 int fc_assignor_clear(fc_assignor *ma);
@@ -214,6 +225,99 @@ int fc_corr_set_profiling(fc_correlator *corr, int enable);
 /* Copies up to max entries; *n receives the number of kernel families. */
 int fc_corr_profile(fc_correlator *corr, fc_kernel_time *out, int max, int *n);
 
+/* ------------------------------------------------------ device catalogs */
+/* Synthetic catalogs written straight into device memory as (n, 4) FP64
+ * x, y, z, w rows, from the counter-based Philox4x32-10 generator keyed by
+ * seed.  The reference draws such catalogs with numpy on the host
+ * (fftcorr/catalog/random_catalog.py); these have no counterpart in it.
+ * Uniform: positions uniform in [lo, hi) per axis, w uniform in
+ * [wmin, wmax) (wmin == wmax: constant). */
+int fc_catalog_uniform(double *posw_device, int64_t n, const double lo[3],
+                       const double hi[3], double wmin, double wmax,
+                       uint64_t seed);
+/* Clustered periodic box [0, boxsize)^3: ncentres uniform centres, each
+ * point a uniformly chosen centre plus an isotropic Gaussian offset of
+ * width sigma, wrapped into the box. */
+int fc_catalog_clustered_box(double *posw_device, int64_t n, double boxsize,
+                             int ncentres, double sigma, double wmin,
+                             double wmax, uint64_t seed);
+/* Uniform in the volume of the shell sector rmin <= r < rmax, |RA| <= ra_half
+ * about +x, |Dec| <= dec_half (radians), observer at the origin; weights
+ * times wsign (-1 gives the negated randoms of a D - alpha R grid). */
+int fc_catalog_sector(double *posw_device, int64_t n, double rmin, double rmax,
+                      double ra_half, double dec_half, double wmin, double wmax,
+                      double wsign, uint64_t seed);
+/* apply_displacement_field (fftcorr/grid/utils.pyx:21-55) on the GPU: out =
+ * pos + disp[cell of pos] for n host positions (n, 3), host field (N0, N1,
+ * N2, 3).  FC_ERR_INVALID if a position has no cell and periodic_wrap is 0. */
+int fc_apply_displacement(const fc_grid *grid, const double *pos, int64_t n,
+                          const double *disp, int periodic_wrap, double *out);
+
+/* ---------------------------------------------------------- batched form */
+/* Many periodic boxes taken through mass assignment (periodic wrap), the
+ * periodic normalisation delta = (rho - mean) / mean of the reference CLI
+ * (cc/fftcorr.cc:369-375) and PeriodicCorrelator::correlate_internal
+ * (cc/correlate/correlator.h:273-357), captured once into one CUDA graph.
+ * Each box's results equal those of MassAssignor + add_scalar/multiply_by +
+ * PeriodicCorrelator run on that box alone (same bits for the same
+ * precision).  The reference runs such boxes one at a time; this batch has
+ * no counterpart in it. */
+typedef struct fc_batch fc_batch;
+typedef struct fc_batch_box {
+  int shape[3];              /* grid cells per axis                       */
+  double cell_size;          /* box edge = shape[i] * cell_size, origin 0 */
+  const double *posw_device; /* (n, 4) FP64 x, y, z, w in device memory;
+                                must stay allocated and unmoved for the
+                                batch's lifetime (the graph reads it)    */
+  int64_t n;
+} fc_batch_box;
+typedef struct fc_batch_params {
+  int scheme;      /* distribution scheme (FC_CLOUD_IN_CELL, ...)         */
+  int window;      /* window correction of the k-subgrid                  */
+  double rmax, dr, kmax, dk;
+  int maxell;      /* 0, 2 or 4                                           */
+  int precision;   /* FC_FP32_MIXED or FC_FP64                            */
+  int lanes;       /* streams of the graph; 0 = from the tuning table     */
+  int tune;        /* 1: time candidates for entries missing from the
+                      tuning table; 0: use fixed defaults for them        */
+} fc_batch_params;
+typedef struct fc_batch_info_t {
+  int nboxes, lanes, hist_blocks;
+  int64_t graph_nodes;       /* nodes of the captured graph               */
+  int64_t kernel_nodes;      /* its kernel nodes (cuFFT and CUB included) */
+  int64_t own_kernel_nodes;  /* of which this library's own kernels      */
+  int64_t hist_items;        /* histogram chunk reductions per replay     */
+  int64_t device_bytes;      /* device memory the batch holds             */
+} fc_batch_info_t;
+int fc_batch_params_default(fc_batch_params *p);
+/* Allocates everything, tunes, captures and instantiates the graph. */
+int fc_batch_create(const fc_batch_box *boxes, int nboxes,
+                    const fc_batch_params *params, fc_batch **out);
+int fc_batch_destroy(fc_batch *batch);
+/* Replays the graph and waits; seconds = its device time. */
+int fc_batch_run(fc_batch *batch, double *seconds);
+/* The two halves of fc_batch_run. */
+int fc_batch_launch(fc_batch *batch);
+int fc_batch_wait(fc_batch *batch, double *seconds);
+int fc_batch_info(const fc_batch *batch, fc_batch_info_t *info);
+int fc_batch_box_dims(const fc_batch *batch, int box, int *nrows, int *nr,
+                      int *nk);
+/* The box's tables after a run, as fc_corr_results. */
+int fc_batch_results(const fc_batch *batch, int box, double *rbins,
+                     int *rcounts, double *rhist, double *kbins, int *kcounts,
+                     double *khist, double *zerolag);
+/* The box's assignment counters, as fc_assignor_stats (times are 0). */
+int fc_batch_box_stats(const fc_batch *batch, int box, fc_assign_stats *s);
+
+/* Launch-tuning table of the batched form (thread and wave counts of the
+ * grid-stride kernels per grid size, lane count, histogram CTAs): the
+ * library's analogue of FFTW wisdom (fftcorr/fftw/fftw.pyx:3-14), written
+ * and read as text lines "kernel precision size a b". */
+int fc_tune_export(const char *path);
+int fc_tune_import(const char *path);
+int fc_tune_forget(void);
+int fc_tune_count(int *n);
+
 /* --------------------------------------------------------- HistogramList */
 typedef struct fc_hist fc_hist;
 
@@ -263,6 +367,7 @@ int fc_host_unregister(void *ptr);
 int fc_device_malloc(size_t bytes, void **ptr);
 int fc_device_free(void *ptr);
 int fc_memcpy_htod(void *dst, const void *src, size_t bytes);
+int fc_memcpy_dtoh(void *dst, const void *src, size_t bytes);
 /* Device-timeline stopwatch: start and stop synchronise the device and
  * record an event on the default stream, so the interval covers all work
  * issued in between on any stream. */

@@ -114,6 +114,29 @@ def grid_coords(pos, posmin, cell, shape, periodic):
     return out if ok else None
 
 
+def apply_displacement_field(pos, disp, posmin, cell, shape, periodic):
+    """out = pos + disp[int(grid coords of pos)] (fftcorr/grid/utils.pyx:21-40);
+    None when a position has no cell (the reference raises ValueError)."""
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    out = np.empty_like(pos)
+    for i in range(pos.shape[0]):
+        x = grid_coords(pos[i], posmin, cell, shape, periodic)
+        if x is None:
+            return None
+        d = disp[int(x[0]), int(x[1]), int(x[2])]
+        for j in range(3):
+            out[i, j] = pos[i, j] + d[j]
+    return out
+
+
+def normalise_periodic(grid, totw):
+    """The CLI's periodic normalisation (cc/fftcorr.cc:369-375): mean =
+    totw / size, then add_scalar(-mean) and multiply_by(1.0 / mean)."""
+    mean = totw / grid.size
+    out = grid + (-mean)
+    return out * (1.0 / mean)
+
+
 def mass_assign(posw, shape, posmin, cell, scheme, periodic=False, grid=None,
                 wave=None):
     """Grid of an (n, 4) posw catalog in input order (buffer_size 0).
