@@ -23,7 +23,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 DEFAULT_REFERENCE = "/root/reference"
 
 SOURCES = ["fc_core.cu", "fc_hist.cu", "fc_assign.cu", "fc_fused.cu", "fc_corr.cu",
-           "fc_batch.cu", "fc_catalog.cu"]
+           "fc_batch.cu", "fc_catalog.cu", "fc_serve.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

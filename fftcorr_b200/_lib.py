@@ -84,6 +84,46 @@ class BatchInfo(ctypes.Structure):
                 ("hist_items", ctypes.c_int64), ("device_bytes", ctypes.c_int64)]
 
 
+class CatalogSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("n", ctypes.c_int64),
+                ("posw", ctypes.c_void_p), ("boxsize", ctypes.c_double),
+                ("ncentres", ctypes.c_int), ("sigma", ctypes.c_double),
+                ("rmin", ctypes.c_double), ("rmax", ctypes.c_double),
+                ("ra_half", ctypes.c_double), ("dec_half", ctypes.c_double),
+                ("wmin", ctypes.c_double), ("wmax", ctypes.c_double),
+                ("wsign", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("shape", ctypes.c_int * 3),
+                ("cell", ctypes.c_double), ("posmin", ctypes.c_double * 3),
+                ("scheme", ctypes.c_int), ("window", ctypes.c_int),
+                ("rmax", ctypes.c_double), ("dr", ctypes.c_double),
+                ("kmax", ctypes.c_double), ("dk", ctypes.c_double),
+                ("maxell", ctypes.c_int), ("precision", ctypes.c_int),
+                ("want_rr", ctypes.c_int), ("data", CatalogSpec),
+                ("randoms", CatalogSpec)]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int),
+                ("queued_s", ctypes.c_double), ("run_s", ctypes.c_double),
+                ("latency_s", ctypes.c_double), ("footprint", ctypes.c_size_t),
+                ("nrows", ctypes.c_int), ("nr", ctypes.c_int), ("nk", ctypes.c_int),
+                ("has_rr", ctypes.c_int), ("data", AssignStats),
+                ("randoms", AssignStats), ("message", ctypes.c_char * 256)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("queued", ctypes.c_int), ("running", ctypes.c_int),
+                ("peak_running", ctypes.c_int), ("resident_objects", ctypes.c_int),
+                ("completed", ctypes.c_uint64),
+                ("admitted_out_of_order", ctypes.c_uint64),
+                ("evictions", ctypes.c_uint64), ("bytes_resident", ctypes.c_size_t),
+                ("bytes_transient", ctypes.c_size_t), ("peak_bytes", ctypes.c_size_t),
+                ("budget", ctypes.c_size_t)]
+
+
 # name -> (restype, argtypes); every fc_* entry returns an fc_status int.
 _SIGNATURES = {
     "fc_last_error": (ctypes.c_char_p, []),
@@ -172,6 +212,23 @@ _SIGNATURES = {
                                          ctypes.c_uint64]),
     "fc_apply_displacement": (ctypes.c_int, [ctypes.c_void_p, c_double_p, ctypes.c_int64,
                                              c_double_p, ctypes.c_int, c_double_p]),
+    "fc_catalog_generate": (ctypes.c_int, [ctypes.POINTER(CatalogSpec), ctypes.c_void_p]),
+    "fc_job_init": (ctypes.c_int, [ctypes.POINTER(Job)]),
+    "fc_job_footprint": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_size_t)]),
+    "fc_server_create": (ctypes.c_int, [ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                        c_void_pp]),
+    "fc_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "fc_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job),
+                                        ctypes.POINTER(ctypes.c_uint64)]),
+    "fc_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
+                                      c_int_p]),
+    "fc_server_job_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.POINTER(JobInfo)]),
+    "fc_server_job_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                             c_double_p, c_int_p, c_double_p, c_double_p,
+                                             c_int_p, c_double_p, c_double_p]),
+    "fc_server_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "fc_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
     "fc_batch_params_default": (ctypes.c_int, [ctypes.POINTER(BatchParams)]),
     "fc_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchBox), ctypes.c_int,
                                        ctypes.POINTER(BatchParams), c_void_pp]),

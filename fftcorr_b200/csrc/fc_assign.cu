@@ -1000,6 +1000,22 @@ void assignor_enqueue_graph(Assignor *a, const double *posw, int64_t n,
   a->stream_override = s;
   a->enqueue_graph(posw, n);
 }
+void assignor_add_device(Assignor *a, const double *posw, int64_t n) {
+  a->add_device_posw(posw, n, cudaMemcpyDeviceToDevice);
+  a->flush();
+  FC_CUDA(cudaStreamSynchronize(a->stream()));
+}
+void assignor_clear(Assignor *a) { a->clear(); }
+bool assignor_has_d12() { return FC_HAVE_D12 != 0; }
+void assignor_stats(Assignor *a, fc_assign_stats *s) { a->stats(s); }
+size_t assignor_bytes(const int shape[3], int64_t n) {
+  // Keys, indices and their sort copies, plus the sort's scratch.
+  int64_t nt = 1;
+  for (int i = 0; i < 3; ++i) nt *= (shape[i] + kTile - 1) / kTile;
+  const bool wide = (uint64_t)nt * kTileCells >= 0xffffffffull;
+  const size_t per = (wide ? 8 : 4) * 2 + 4 * 2 + 8;
+  return (size_t)std::max<int64_t>(n, 1) * per + (size_t)nt * 8 + (1 << 20);
+}
 const double *assignor_totals(const Assignor *a) { return a->totals.as<double>(); }
 const unsigned long long *assignor_counts(const Assignor *a) {
   return a->counts.as<unsigned long long>();

@@ -161,6 +161,54 @@ __global__ void k_sector(double *__restrict__ posw, int64_t first, int64_t n,
   }
 }
 
+__device__ __forceinline__ bool in_sector(double x, double y, double z,
+                                          double rmin, double rmax, double ra,
+                                          double sdec) {
+  const double r = sqrt(x * x + y * y + z * z);
+  if (!(r >= rmin && r < rmax)) return false;
+  if (fabs(atan2(y, x)) > ra) return false;
+  return fabs(z) <= sdec * r;
+}
+
+// Clustered points in the sector: a uniformly chosen centre (from k_sector)
+// plus N(0, sigma^2 I), redrawn until inside the sector (at most 64 draws;
+// then the centre itself).
+__global__ void k_sector_clustered(double *__restrict__ posw, int64_t n,
+                                   const double *__restrict__ centres, int nc,
+                                   double sigma, double rmin, double rmax,
+                                   double ra, double dec, double w0, double w1,
+                                   double wsign, uint64_t seed) {
+  const double sdec = sin(dec);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const U4 a = philox((uint64_t)i, kStreamMember, seed);
+    int ci = (int)(u53(a.v[0], a.v[1]) * nc);
+    if (ci >= nc) ci = nc - 1;
+    const double *c = centres + 4 * ci;
+    double x = c[0], y = c[1], z = c[2];
+    for (uint32_t t = 0; t < 64; ++t) {
+      const U4 b = philox((uint64_t)i, 16 + 2 * t, seed);
+      const U4 d = philox((uint64_t)i, 17 + 2 * t, seed);
+      double z0, z1, z2, z3;
+      box_muller(u53(b.v[0], b.v[1]), u53(b.v[2], b.v[3]), &z0, &z1);
+      box_muller(u53(d.v[0], d.v[1]), u53(d.v[2], d.v[3]), &z2, &z3);
+      const double px = c[0] + sigma * z0, py = c[1] + sigma * z1,
+                   pz = c[2] + sigma * z2;
+      if (in_sector(px, py, pz, rmin, rmax, ra, sdec)) {
+        x = px;
+        y = py;
+        z = pz;
+        break;
+      }
+    }
+    double *p = posw + 4 * i;
+    p[0] = x;
+    p[1] = y;
+    p[2] = z;
+    p[3] = wsign * (w0 == w1 ? w0 : w0 + (w1 - w0) * u53(a.v[2], a.v[3]));
+  }
+}
+
 // out = pos + disp[cell of pos] (utils.pyx:21-40); flag[0] = 1 when a
 // position has no cell (outside the grid without periodic wrap).
 __global__ void k_displace(const double *__restrict__ pos, int stride,
@@ -211,6 +259,66 @@ void catalog_uniform(double *posw, int64_t first, int64_t n, const double lo[3],
                                           make_double3(hi[0], hi[1], hi[2]), w0,
                                           w1, seed);
   FC_LAUNCH_CHECK();
+}
+
+void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s) {
+  const int64_t n = c.n;
+  if (n <= 0) return;
+  switch (c.kind) {
+    case FC_CAT_DEVICE:
+      FC_REQUIRE(c.posw, FC_ERR_INVALID, "null particle array");
+      FC_CUDA(cudaMemcpyAsync(posw, c.posw, (size_t)n * 32,
+                              cudaMemcpyDeviceToDevice, s));
+      return;
+    case FC_CAT_HOST:
+      FC_REQUIRE(c.posw, FC_ERR_INVALID, "null particle array");
+      FC_CUDA(cudaMemcpyAsync(posw, c.posw, (size_t)n * 32,
+                              cudaMemcpyHostToDevice, s));
+      return;
+    case FC_CAT_UNIFORM_BOX: {
+      const double lo[3] = {0, 0, 0};
+      const double hi[3] = {c.boxsize, c.boxsize, c.boxsize};
+      catalog_uniform(posw, 0, n, lo, hi, c.wmin, c.wmax, c.seed, s);
+      return;
+    }
+    case FC_CAT_CLUSTERED_BOX: {
+      FC_REQUIRE(c.ncentres > 0, FC_ERR_INVALID, "ncentres must be positive");
+      // Stream-ordered scratch: no device-wide synchronisation.
+      double *centres = nullptr;
+      FC_CUDA(cudaMallocAsync(&centres, (size_t)c.ncentres * 3 * sizeof(double), s));
+      k_centres<<<gen_blocks(c.ncentres), 256, 0, s>>>(centres, c.ncentres,
+                                                       c.boxsize, c.seed);
+      FC_LAUNCH_CHECK();
+      k_clustered<<<gen_blocks(n), 256, 0, s>>>(posw, 0, n, centres, c.ncentres,
+                                                c.boxsize, c.sigma, c.wmin,
+                                                c.wmax, c.seed);
+      FC_LAUNCH_CHECK();
+      FC_CUDA(cudaFreeAsync(centres, s));
+      return;
+    }
+    case FC_CAT_SECTOR_UNIFORM:
+      k_sector<<<gen_blocks(n), 256, 0, s>>>(posw, 0, n, c.rmin, c.rmax,
+                                             c.ra_half, c.dec_half, c.wmin,
+                                             c.wmax, c.wsign, c.seed);
+      FC_LAUNCH_CHECK();
+      return;
+    case FC_CAT_SECTOR_CLUSTERED: {
+      FC_REQUIRE(c.ncentres > 0, FC_ERR_INVALID, "ncentres must be positive");
+      double *centres = nullptr;
+      FC_CUDA(cudaMallocAsync(&centres, (size_t)c.ncentres * 4 * sizeof(double), s));
+      k_sector<<<gen_blocks(c.ncentres), 256, 0, s>>>(
+          centres, 0, c.ncentres, c.rmin, c.rmax, c.ra_half, c.dec_half, 1.0,
+          1.0, 1.0, c.seed ^ 0x3c6ef372fe94f82bull);
+      FC_LAUNCH_CHECK();
+      k_sector_clustered<<<gen_blocks(n), 256, 0, s>>>(
+          posw, n, centres, c.ncentres, c.sigma, c.rmin, c.rmax, c.ra_half,
+          c.dec_half, c.wmin, c.wmax, c.wsign, c.seed);
+      FC_LAUNCH_CHECK();
+      FC_CUDA(cudaFreeAsync(centres, s));
+      return;
+    }
+  }
+  FC_THROW(FC_ERR_INVALID, "unknown catalog kind");
 }
 
 void displace(const double *pos, int stride, int64_t n, const double *disp,
@@ -274,6 +382,16 @@ int fc_catalog_sector(double *posw_device, int64_t n, double rmin, double rmax,
     k_sector<<<gen_blocks(n), 256>>>(posw_device, 0, n, rmin, rmax, ra_half,
                                     dec_half, wmin, wmax, wsign, seed);
     FC_LAUNCH_CHECK();
+    FC_CUDA(cudaStreamSynchronize(0));
+  });
+}
+
+int fc_catalog_generate(const fc_catalog_spec *spec, double *posw_device) {
+  return guard([&] {
+    FC_REQUIRE(spec, FC_ERR_INVALID, "null argument");
+    FC_REQUIRE(spec->n >= 0, FC_ERR_INVALID, "negative count");
+    FC_REQUIRE(spec->n == 0 || posw_device, FC_ERR_INVALID, "null output");
+    catalog_generate(*spec, posw_device, 0);
     FC_CUDA(cudaStreamSynchronize(0));
   });
 }

@@ -946,6 +946,14 @@ Correlator *correlator_new(int kind, const int shape[3], double cell,
   return c;
 }
 void correlator_delete(Correlator *c) { delete c; }
+void correlator_autocorrelate(Correlator *c, const Grid *g) {
+  for (int i = 0; i < 3; ++i)
+    FC_REQUIRE(g->shape[i] == c->geo.shape[i], FC_ERR_INVALID,
+               "grid shape does not match the correlator");
+  stream_after(c->stream, g->stream);
+  c->enqueue(g->ptr(), false);
+  c->synchronize();
+}
 void correlator_make_deferred(Correlator *c) { c->make_deferred(); }
 void *correlator_work(Correlator *c) { return c->work.get(); }
 void correlator_set_stream(Correlator *c, cudaStream_t s) { c->set_stream(s); }
@@ -993,16 +1001,25 @@ void correlator_time_kernels(Correlator *c, int which, cudaStream_t s) {
 size_t correlator_footprint(int kind, const int shape[3], double cell,
                             double rmax, double kmax, int maxell,
                             int precision) {
-  (void)maxell;
-  Geometry g(shape, cell, FC_NO_CORRECTION, rmax, rmax, kmax, kmax, 0);
+  Geometry g(shape, cell, FC_NO_CORRECTION, rmax, rmax, kmax, kmax, maxell);
   const size_t rb = precision == FC_FP64 ? 8 : 4;
-  size_t bytes = g.nreal_padded() * rb;         // work
-  bytes += g.ncomplex() * 2 * rb;               // grid2 FFT
-  bytes += g.ncomplex() * 2 * rb;               // cuFFT work area (estimate)
-  bytes += g.ncells() * 8;                      // host-input staging
-  bytes += g.rcells() * (8 + 4) + g.kcells() * (8 + 4);  // subgrids + perms
-  (void)kind;
-  return bytes;
+  const size_t eb = 2 * rb;
+  size_t bytes = 0;
+  const char *mode = std::getenv("FFTCORR_B200_FFT");
+  const bool want_fused = !(mode && std::string(mode) == "cufft");
+  if (kind == FC_SURVEY && want_fused && FusedSurvey::supported(g.shape, g.rsize)) {
+    const size_t h = g.shape[2] / 2 + 1;
+    bytes += 2 * g.ncomplex() * eb;                          // W, G
+    bytes += (size_t)g.rsize * g.shape[1] * h * eb;          // Wr
+    bytes += (size_t)g.rsize * g.rsize * h * eb;             // Wry
+    if (precision != FC_FP64) bytes += g.ncells() * 4;       // FP32 density
+  } else {
+    bytes += g.nreal_padded() * rb;                          // work
+    if (kind == FC_SURVEY) bytes += g.ncomplex() * eb;       // grid2 FFT
+    bytes += g.ncomplex() * eb;                              // cuFFT work area
+  }
+  bytes += g.rcells() * (8 + 4) + g.kcells() * (8 + 4);    // subgrids + perms
+  return bytes + (4 << 20);
 }
 
 }  // namespace fc

@@ -89,6 +89,8 @@ struct AssignGeomLite {
 void catalog_uniform(double *posw, int64_t first, int64_t n, const double lo[3],
                      const double hi[3], double w0, double w1, uint64_t seed,
                      cudaStream_t s);
+// Writes the catalog a spec describes into posw (n rows of x, y, z, w).
+void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s);
 // out[i] = pos[i] + disp[cell of pos[i]]; *flag = 1 if some position has no
 // cell.  Rows of pos and out are `stride` / `out_stride` doubles apart.
 void displace(const double *pos, int stride, int64_t n, const double *disp,
@@ -105,6 +107,14 @@ void assignor_delete(Assignor *a);
 void assignor_prepare_graph(Assignor *a, int64_t max_n, cudaStream_t s);
 void assignor_enqueue_graph(Assignor *a, const double *posw, int64_t n,
                             cudaStream_t s);
+// Assigns n particles from a device array and waits (MassAssignor::
+// add_particles_to_buffer + flush).
+void assignor_add_device(Assignor *a, const double *posw, int64_t n);
+void assignor_clear(Assignor *a);
+bool assignor_has_d12();
+void assignor_stats(Assignor *a, fc_assign_stats *s);
+// Device bytes an assignor holds after assigning n particles at once.
+size_t assignor_bytes(const int shape[3], int64_t n);
 const double *assignor_totals(const Assignor *a);  // device [totw, totwsq]
 const unsigned long long *assignor_counts(const Assignor *a);  // [num_added]
 
@@ -114,6 +124,10 @@ Correlator *correlator_new(int kind, const int shape[3], double cell,
                            double dr, double kmax, double dk, int maxell,
                            int precision);
 void correlator_delete(Correlator *c);
+// Autocorrelation of a device grid (waits for the result).
+void correlator_autocorrelate(Correlator *c, const Grid *g);
+size_t correlator_footprint(int kind, const int shape[3], double cell,
+                            double rmax, double kmax, int maxell, int precision);
 // Periodic correlators only: every multipole keeps its own subgrids and the
 // histograms are left to the caller (correlator_hist_work).
 void correlator_make_deferred(Correlator *c);

@@ -247,11 +247,101 @@ int fc_catalog_clustered_box(double *posw_device, int64_t n, double boxsize,
 int fc_catalog_sector(double *posw_device, int64_t n, double rmin, double rmax,
                       double ra_half, double dec_half, double wmin, double wmax,
                       double wsign, uint64_t seed);
+/* A catalog described by value, for fc_catalog_generate and the serving
+ * form: copied from device or host memory, or generated from a seed. */
+enum {
+  FC_CAT_DEVICE = 0,          /* posw: device (n, 4) array                 */
+  FC_CAT_HOST = 1,            /* posw: host (n, 4) array                   */
+  FC_CAT_UNIFORM_BOX = 2,     /* uniform in [0, boxsize)^3                 */
+  FC_CAT_CLUSTERED_BOX = 3,   /* as fc_catalog_clustered_box               */
+  FC_CAT_SECTOR_UNIFORM = 4,  /* as fc_catalog_sector                      */
+  FC_CAT_SECTOR_CLUSTERED = 5 /* ncentres uniform in the sector, each point
+                                 a centre plus N(0, sigma^2 I), redrawn until
+                                 inside the sector                         */
+};
+typedef struct fc_catalog_spec {
+  int kind;
+  int64_t n;
+  const double *posw;         /* FC_CAT_DEVICE / FC_CAT_HOST               */
+  double boxsize;             /* box kinds                                 */
+  int ncentres;
+  double sigma;
+  double rmin, rmax, ra_half, dec_half;  /* sector kinds (radians)       */
+  double wmin, wmax, wsign;   /* weights wsign * U[wmin, wmax)             */
+  uint64_t seed;
+} fc_catalog_spec;
+int fc_catalog_generate(const fc_catalog_spec *spec, double *posw_device);
 /* apply_displacement_field (fftcorr/grid/utils.pyx:21-55) on the GPU: out =
  * pos + disp[cell of pos] for n host positions (n, 3), host field (N0, N1,
  * N2, 3).  FC_ERR_INVALID if a position has no cell and periodic_wrap is 0. */
 int fc_apply_displacement(const fc_grid *grid, const double *pos, int64_t n,
                           const double *disp, int periodic_wrap, double *out);
+
+/* ---------------------------------------------------------- serving form */
+/* A request loop over correlation jobs with continuous batching: `slots`
+ * workers each take the first queued job that fits the HBM budget, so jobs
+ * arriving while others run start as soon as a slot and memory free up and
+ * overlap on the device; grids, assignors and correlators (FFT plans, bin
+ * indices) stay resident by configuration and are reused, idle ones evicted
+ * least recently used first.  A job is one catalog's run of the reference
+ * CLI (cc/fftcorr.cc:233-463): periodic: assign, delta = (rho - mean)/mean,
+ * autocorrelate; survey: NN = D - alpha R (alpha = sum w_D / sum w_R, the
+ * randoms negated as fftcorr/fftcorr.py:538 does), autocorrelate, and with
+ * want_rr also the RR grid.  Results equal a job run alone.  Has no
+ * counterpart in the reference. */
+typedef struct fc_job {
+  int kind;                 /* FC_PERIODIC or FC_SURVEY                    */
+  int shape[3];
+  double cell;
+  double posmin[3];         /* survey: grid origin (observer at 0)         */
+  int scheme, window;
+  double rmax, dr, kmax, dk;
+  int maxell, precision;
+  int want_rr;              /* survey: also correlate RR (for xi)          */
+  fc_catalog_spec data;     /* host / device catalogs must stay valid until
+                               the job completes                           */
+  fc_catalog_spec randoms;  /* survey only                                 */
+} fc_job;
+typedef struct fc_job_info {
+  int state;                /* 0 queued, 1 running, 2 done                 */
+  int status;               /* fc_status of a finished job                 */
+  double queued_s, run_s, latency_s;  /* submit->start, start->end,
+                                         submit->end (host clock)          */
+  size_t footprint;         /* admission estimate, bytes                   */
+  int nrows, nr, nk, has_rr;
+  fc_assign_stats data, randoms;
+  char message[256];        /* error message of a failed job               */
+} fc_job_info;
+typedef struct fc_server_stats {
+  int queued, running, peak_running, resident_objects;
+  uint64_t completed, admitted_out_of_order, evictions;
+  size_t bytes_resident, bytes_transient, peak_bytes, budget;
+} fc_server_stats_t;
+typedef struct fc_server fc_server;
+int fc_job_init(fc_job *job);
+/* Device bytes the job needs (FC_ERR_INVALID for a malformed job). */
+int fc_job_footprint(const fc_job *job, size_t *bytes);
+/* max_bypass: how many times a waiting job may be passed by later jobs
+ * that fit when it does not (0: strict arrival order). */
+int fc_server_create(size_t hbm_budget, int slots, int max_bypass,
+                     fc_server **out);
+/* Waits for running jobs and frees everything. */
+int fc_server_destroy(fc_server *server);
+/* Queues a job; FC_ERR_ADMISSION if it alone exceeds the budget. */
+int fc_server_submit(fc_server *server, const fc_job *job, uint64_t *ticket);
+/* Waits up to timeout_s (< 0: forever); *done = 1 when it finished. */
+int fc_server_wait(fc_server *server, uint64_t ticket, double timeout_s,
+                   int *done);
+int fc_server_job_info(fc_server *server, uint64_t ticket, fc_job_info *info);
+/* Tables of a finished job: which 0 = NN (or the periodic grid), 1 = RR;
+ * arrays as fc_corr_results.  A failed job returns its status. */
+int fc_server_job_results(fc_server *server, uint64_t ticket, int which,
+                          double *rbins, int *rcounts, double *rhist,
+                          double *kbins, int *kcounts, double *khist,
+                          double *zerolag);
+/* Forgets a finished job's results. */
+int fc_server_release(fc_server *server, uint64_t ticket);
+int fc_server_stats(fc_server *server, fc_server_stats_t *stats);
 
 /* ---------------------------------------------------------- batched form */
 /* Many periodic boxes taken through mass assignment (periodic wrap), the
