@@ -55,6 +55,12 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-boxes", type=int, default=64)
     ap.add_argument("--only-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--only-served", action="store_true")
+    ap.add_argument("--served-jobs", type=int, default=24)
+    ap.add_argument("--served-slots", type=int, default=3)
+    ap.add_argument("--mix-jobs", type=int, default=48)
+    ap.add_argument("--mix-rate", type=float, default=6.0)
     return ap.parse_args()
 
 
@@ -394,6 +400,151 @@ def run_batched(a, timed_fn):
             "particles": npart, "cells": cells, "forms": out}
 
 
+# ----------------------------------------------------------- served form
+
+def _pct(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def survey_job_spec(w, seed, precision, nd=None, nr=None, ngrid=None, maxell=None,
+                    want_rr=True):
+    """The headline survey job as a served request: clustered data and
+    uniform randoms in the sector, generated on the device from seeds."""
+    from fftcorr_b200 import mocks
+    from fftcorr_b200.correlate import TSC_ALIASED_CORRECTION
+    from fftcorr_b200.particle_mesh import DistributionScheme
+    from fftcorr_b200.serve import (CAT_SECTOR_CLUSTERED, CAT_SECTOR_UNIFORM,
+                                    JobSpec, catalog_spec)
+    ngrid = ngrid or w.ngrid
+    posmin, cell = mocks.survey_box(w.sector, w.rmax, ngrid)
+    data = catalog_spec(CAT_SECTOR_CLUSTERED, n=nd or w.nd, ncentres=10000, sigma=5.0,
+                        wmin=0.5, wmax=1.5, seed=seed)
+    rand = catalog_spec(CAT_SECTOR_UNIFORM, n=nr or w.nr, wmin=0.5, wmax=1.5,
+                        seed=seed + 1)
+    return JobSpec("survey", ngrid, cell, data, rand, posmin=posmin,
+                   scheme=DistributionScheme.TRIANGULAR_SHAPED_CLOUD,
+                   window=TSC_ALIASED_CORRECTION, rmax=w.rmax, dr=w.dr,
+                   kmax=w.kmax, dk=w.dk,
+                   maxell=w.maxell if maxell is None else maxell,
+                   precision=precision, want_rr=want_rr)
+
+
+def served_budget():
+    """180 GB, or the free device memory less a margin when that is less."""
+    from fftcorr_b200 import _lib
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    _lib.call("fc_device_memory", ctypes.byref(free), ctypes.byref(total))
+    return int(min(180 * 10**9, free.value - (6 << 30)))
+
+
+def run_served_saturated(a, w, precision, timer):
+    """All requests queued at once: device-timed throughput of the server."""
+    from fftcorr_b200.serve import Server
+    srv = Server(served_budget(), slots=a.served_slots)
+    warm = survey_job_spec(w, 900, precision)
+    srv.wait(srv.submit(warm))
+    specs = [survey_job_spec(w, 1000 + 10 * i, precision) for i in range(a.served_jobs)]
+    timer.start()
+    tickets = [srv.submit(s) for s in specs]
+    for t in tickets:
+        srv.wait(t)
+    secs = timer.stop()
+    lat = [srv.info(t)["latency_s"] for t in tickets]
+    run = [srv.info(t)["run_s"] for t in tickets]
+    bad = [srv.info(t)["message"] for t in tickets if srv.info(t)["status"] != 0]
+    st = srv.stats()
+    srv.close()
+    return {"value": len(specs) / secs, "unit": "jobs/s", "jobs": len(specs),
+            "slots": a.served_slots, "device_s": secs,
+            "p50_latency_s": _pct(lat, 50), "p99_latency_s": _pct(lat, 99),
+            "mean_run_s": float(np.mean(run)), "peak_running": st["peak_running"],
+            "peak_bytes": st["peak_bytes"], "errors": bad}
+
+
+def snap7(n):
+    """Nearest even 7-smooth integer (2^a 3^b 5^c 7^d)."""
+    best = None
+    for m in range(max(2, n - 64), n + 65):
+        if m % 2:
+            continue
+        k = m
+        for p in (2, 3, 5, 7):
+            while k % p == 0:
+                k //= p
+        if k == 1 and (best is None or abs(m - n) < abs(best - n)):
+            best = m
+    return best
+
+
+def mix_job(w, i, rng):
+    from fftcorr_b200.particle_mesh import DistributionScheme
+    from fftcorr_b200.serve import CAT_CLUSTERED_BOX, JobSpec, catalog_spec
+    n = snap7(int(round(np.exp(rng.uniform(np.log(64), np.log(1024))))))
+    maxell = int(rng.choice([0, 2, 4]))
+    npart = int(np.exp(rng.uniform(np.log(0.1e6), np.log(50e6))))
+    want_rr = bool(rng.random() < 0.5)      # xi job (NN and RR) or P job (NN)
+    if rng.random() < 0.5:
+        L = float(rng.uniform(1000.0, 2000.0))
+        data = catalog_spec(CAT_CLUSTERED_BOX, n=npart, boxsize=L, ncentres=10000,
+                            sigma=5.0, seed=5000 + i)
+        spec = JobSpec("periodic", (n, n, n), L / n, data,
+                       scheme=DistributionScheme.CLOUD_IN_CELL, rmax=200.0, dr=5.0,
+                       kmax=0.1, dk=0.005, maxell=maxell, precision="fp32")
+        return spec, ("periodic", n, maxell, npart)
+    nd = max(1, npart // 5)
+    spec = survey_job_spec(w, 5000 + 7 * i, "fp32", nd=nd, nr=npart, ngrid=(n, n, n),
+                           maxell=maxell, want_rr=want_rr)
+    return spec, ("survey", n, maxell, npart)
+
+
+def run_served_mix(a, w):
+    """Poisson arrivals of mixed periodic / survey, xi / P jobs."""
+    from fftcorr_b200.serve import Server
+    rng = np.random.default_rng(5)
+    jobs = [mix_job(w, i, rng) for i in range(a.mix_jobs)]
+    gaps = rng.exponential(1.0 / a.mix_rate, len(jobs))
+    srv = Server(served_budget(), slots=a.served_slots)
+    t0 = time.perf_counter()
+    tickets = []
+    due = t0
+    for (spec, _), gap in zip(jobs, gaps):
+        due += gap
+        delay = due - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        tickets.append(srv.submit(spec))
+    for t in tickets:
+        srv.wait(t)
+    wall = time.perf_counter() - t0
+    infos = [srv.info(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    lat = [i["latency_s"] for i in infos]
+    return {"value": len(jobs) / wall, "unit": "jobs/s (host wall clock)",
+            "jobs": len(jobs), "arrival_rate_per_s": a.mix_rate,
+            "p50_latency_s": _pct(lat, 50), "p99_latency_s": _pct(lat, 99),
+            "max_latency_s": max(lat), "slots": a.served_slots,
+            "peak_running": st["peak_running"], "peak_bytes": st["peak_bytes"],
+            "budget": st["budget"], "evictions": st["evictions"],
+            "admitted_out_of_order": st["admitted_out_of_order"],
+            "errors": [i["message"] for i in infos if i["status"] != 0],
+            "mix": "N^3 log-uniform [64^3, 1024^3] snapped to even 7-smooth, "
+                   "ell_max from {0,2,4}, periodic/survey 50/50, Np log-uniform "
+                   "[0.1M, 50M], xi (NN+RR) / P (NN) 50/50, FP32-mixed, seed 5"}
+
+
+def run_served(a, w, timer):
+    out = {"workload_512": "served survey xi_ell+P_ell jobs at 512^3, ell<=4, "
+                           "20M clustered data + 100M randoms generated on the "
+                           "device per job, all queued at once"}
+    out["fp32"] = run_served_saturated(a, w, "fp32", timer)
+    if not a.no_fp64:
+        out["fp64"] = run_served_saturated(a, w, "fp64", timer)
+        out["fp32_over_fp64"] = out["fp32"]["value"] / out["fp64"]["value"]
+    out["mix"] = run_served_mix(a, w)
+    return out
+
+
 # --------------------------------------------------------- CPU baseline
 
 def cpu_baseline_sample(w, R, threads):
@@ -501,6 +652,11 @@ def main():
             print(json.dumps({"batched": run_batched(a, None)}))
         dist.close()
         return
+    if a.only_served:
+        if rank == 0:
+            print(json.dumps({"served": run_served(a, Workload(a), DeviceTimer())}))
+        dist.close()
+        return
     w = Workload(a)
     t_gen = time.perf_counter()
     D, R = w.catalogs(seed_offset=rank)
@@ -587,6 +743,7 @@ def main():
                             if tuple(w.ngrid) == (512, 512, 512) else None)}
 
     batched = None if a.no_batched else run_batched(a, None)
+    served = None if a.no_served else run_served(a, w, timer)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -620,6 +777,7 @@ def main():
             "gpu_launches": launches_dev,
             "catalog_generation_s": t_gen,
             "batched": batched,
+            "served": served,
         }
         print(json.dumps(line))
     for p in (dD, dR):

@@ -111,7 +111,8 @@ class JobInfo(ctypes.Structure):
                 ("latency_s", ctypes.c_double), ("footprint", ctypes.c_size_t),
                 ("nrows", ctypes.c_int), ("nr", ctypes.c_int), ("nk", ctypes.c_int),
                 ("has_rr", ctypes.c_int), ("data", AssignStats),
-                ("randoms", AssignStats), ("message", ctypes.c_char * 256)]
+                ("randoms", AssignStats), ("phase_s", ctypes.c_double * 8),
+                ("message", ctypes.c_char * 256)]
 
 
 class ServerStats(ctypes.Structure):
@@ -195,6 +196,8 @@ _SIGNATURES = {
     "fc_device_free": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_memcpy_htod": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "fc_memcpy_dtoh": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    "fc_device_memory": (ctypes.c_int, [ctypes.POINTER(ctypes.c_size_t),
+                                        ctypes.POINTER(ctypes.c_size_t)]),
     "fc_timer_create": (ctypes.c_int, [c_void_pp]),
     "fc_timer_start": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_timer_stop": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),

@@ -354,12 +354,40 @@ __global__ void __launch_bounds__(kScatterThreads)
 }
 
 // K-scatter for stencils of width <= 3 (NGP, CIC, TSC): one thread per
-// home cell of the 8x8x8 tile.  Each thread walks its cell's particles in
-// sorted order and accumulates the W^3 products wx[a]*wy[b]*wz[c] of every
-// particle in registers (S_h[a][b][c]); the sums go to shared memory, and
-// every footprint cell then adds the S_h[o] of the home cells h = f - o in a
-// fixed order.  Per particle this is one gather of its position and W^3
-// register operations, instead of W^3 shared-memory walks.
+// home cell of the 8x8x8 tile.  The tile's particles (contiguous in sorted
+// order) are staged in chunks: all threads gather positions and weights in
+// parallel into shared memory (fractional cell offsets and weight), then
+// each thread walks its own cell's particles of the chunk in sorted order
+// and accumulates the W^3 products wx[a]*wy[b]*wz[c] in registers
+// (S_h[a][b][c]).  The sums go to shared memory, and every footprint cell
+// then adds the S_h[o] of the home cells h = f - o in a fixed order.  Each
+// cell's particles are summed in sorted order whatever the chunking, so the
+// grid is the same bits on every run.
+template <int S>
+struct ScatterS {
+  static constexpr int W = Stencil<S>::W;
+  static constexpr int W3 = W * W * W;
+  static constexpr int F = kTile + W - 1;
+  static constexpr int F3 = F * F * F;
+  // Staged particles per chunk: at least 1024, more when the S_h buffer the
+  // chunk shares memory with is larger (TSC).
+  static constexpr int C0 = (W3 * kTileCells * 8) / 36 / 32 * 32;
+  static constexpr int C = C0 > 1024 ? C0 : 1024;
+  static constexpr size_t region =
+      (size_t)W3 * kTileCells * 8 > (size_t)C * 36 ? (size_t)W3 * kTileCells * 8
+                                                   : (size_t)C * 36;
+  static constexpr size_t smem = region + (size_t)F3 * 8;
+};
+
+__device__ __forceinline__ int lower_bound_smem(const int *a, int n, int v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
 template <int S, typename KeyT>
 __global__ void __launch_bounds__(kTileCells)
     k_scatter_s(const double *__restrict__ posw, const KeyT *__restrict__ keys,
@@ -367,14 +395,18 @@ __global__ void __launch_bounds__(kTileCells)
                 const uint32_t *__restrict__ tile_start,
                 const uint32_t *__restrict__ tiles, AssignGeom g,
                 double *__restrict__ grid) {
-  constexpr int W = Stencil<S>::W;
+  using Q = ScatterS<S>;
+  constexpr int W = Q::W;
   constexpr int OMIN = Stencil<S>::OMIN;
-  constexpr int W3 = W * W * W;
-  constexpr int F = kTile + W - 1;
-  constexpr int F3 = F * F * F;
+  constexpr int W3 = Q::W3;
+  constexpr int F = Q::F;
+  constexpr int F3 = Q::F3;
+  constexpr int C = Q::C;
   extern __shared__ double smem[];
-  double *sh = smem;              // [W3][512]
-  double *acc = smem + W3 * kTileCells;  // [F3]
+  double *sh = smem;                                   // [W3][512], last
+  double *pd = smem;                                   // [C][4], per chunk
+  int *pc = reinterpret_cast<int *>(smem + 4 * C);     // [C], per chunk
+  double *acc = smem + Q::region / 8;                  // [F3]
 
   const uint32_t tile = tiles[blockIdx.x];
   const uint32_t ts = tile_start[tile];
@@ -384,43 +416,44 @@ __global__ void __launch_bounds__(kTileCells)
   const int ty = (tile / g.nt[2]) % g.nt[1];
   const int tx = tile / (g.nt[2] * g.nt[1]);
   const int o0 = tx * kTile, o1 = ty * kTile, o2 = tz * kTile;
-
-  // This thread's home cell and its particle range [cs, ce).
   const int h = threadIdx.x;
   const KeyT kbase = (KeyT)tile * kTileCells;
-  uint32_t lo = ts, hi = te;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (keys[mid] < kbase + h) lo = mid + 1; else hi = mid;
-  }
-  const uint32_t cs = lo;
-  hi = te;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (keys[mid] < kbase + h + 1) lo = mid + 1; else hi = mid;
-  }
-  const uint32_t ce = lo;
+
   double sacc[W3];
 #pragma unroll
   for (int o = 0; o < W3; ++o) sacc[o] = 0.0;
-  for (uint32_t q = cs; q < ce; ++q) {
-    const double *p = posw + 4 * (size_t)vals[q];
-    double x[3];
-    dev_grid_coords(p, g, x);
-    const int ix = home_cell(x[0], g.n[0]);
-    const int iy = home_cell(x[1], g.n[1]);
-    const int iz = home_cell(x[2], g.n[2]);
-    double wx[W], wy[W], wz[W];
-    Stencil<S>::weights(x[0] - ix, x[1] - iy, x[2] - iz, p[3], wx, wy, wz);
+  for (uint32_t c0 = ts; c0 < te; c0 += C) {
+    const int m = (int)min((uint32_t)C, te - c0);
+    if (c0 != ts) __syncthreads();  // the previous chunk has been consumed
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      const uint32_t q = c0 + i;
+      const double *p = posw + 4 * (size_t)vals[q];
+      double x[3];
+      dev_grid_coords(p, g, x);
+      pd[4 * i + 0] = x[0] - home_cell(x[0], g.n[0]);
+      pd[4 * i + 1] = x[1] - home_cell(x[1], g.n[1]);
+      pd[4 * i + 2] = x[2] - home_cell(x[2], g.n[2]);
+      pd[4 * i + 3] = p[3];
+      pc[i] = (int)(keys[q] - kbase);
+    }
+    __syncthreads();
+    const int lo = lower_bound_smem(pc, m, h);
+    const int hi = lower_bound_smem(pc, m, h + 1);
+    for (int i = lo; i < hi; ++i) {
+      double wx[W], wy[W], wz[W];
+      Stencil<S>::weights(pd[4 * i + 0], pd[4 * i + 1], pd[4 * i + 2],
+                          pd[4 * i + 3], wx, wy, wz);
 #pragma unroll
-    for (int a = 0; a < W; ++a)
+      for (int a = 0; a < W; ++a)
 #pragma unroll
-      for (int b = 0; b < W; ++b) {
-        const double wxy = wx[a] * wy[b];
+        for (int b = 0; b < W; ++b) {
+          const double wxy = wx[a] * wy[b];
 #pragma unroll
-        for (int c = 0; c < W; ++c) sacc[(a * W + b) * W + c] += wxy * wz[c];
-      }
+          for (int c = 0; c < W; ++c) sacc[(a * W + b) * W + c] += wxy * wz[c];
+        }
+    }
   }
+  __syncthreads();  // the chunk buffer becomes S_h
 #pragma unroll
   for (int o = 0; o < W3; ++o) sh[o * kTileCells + h] = sacc[o];
   __syncthreads();
@@ -472,9 +505,7 @@ __global__ void __launch_bounds__(kTileCells)
 
 template <int S>
 size_t scatter_s_smem() {
-  constexpr int W = Stencil<S>::W;
-  constexpr int F = kTile + W - 1;
-  return sizeof(double) * (W * W * W * kTileCells + F * F * F);
+  return ScatterS<S>::smem;
 }
 
 template <int S>

@@ -449,6 +449,15 @@ int fc_memcpy_htod(void *dst, const void *src, size_t bytes) {
   });
 }
 
+int fc_device_memory(size_t *free_bytes, size_t *total_bytes) {
+  return guard([&] {
+    size_t f = 0, t = 0;
+    FC_CUDA(cudaMemGetInfo(&f, &t));
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+  });
+}
+
 int fc_memcpy_dtoh(void *dst, const void *src, size_t bytes) {
   return guard([&] {
     FC_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));

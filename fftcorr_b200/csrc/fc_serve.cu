@@ -79,6 +79,7 @@ struct Job {
   Tables nn, rr;
   bool has_rr = false;
   fc_assign_stats data_stats{}, rand_stats{};
+  double phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   // Resources held while running.
   std::vector<Resident *> held;
   size_t transient = 0;
@@ -160,13 +161,21 @@ struct Server {
   uint64_t completed = 0, admitted_out_of_order = 0, evictions = 0;
   bool stopping = false;
   std::vector<std::thread> workers;
+  // Per-worker catalog staging, kept between jobs (grows only; accounted in
+  // bytes_resident).
+  std::vector<std::unique_ptr<DeviceBuffer>> stage;
+  std::vector<size_t> stage_bytes;
 
   Server(size_t budget_, int slots_, int max_bypass_)
       : budget(budget_), slots(slots_), max_bypass(max_bypass_) {
     FC_REQUIRE(slots >= 1 && slots <= 64, FC_ERR_INVALID, "slots must be 1..64");
     FC_REQUIRE(budget > 0, FC_ERR_INVALID, "budget must be positive");
     FC_CUDA(cudaGetDevice(&device));
-    for (int i = 0; i < slots; ++i) workers.emplace_back([this] { worker(); });
+    for (int i = 0; i < slots; ++i) {
+      stage.emplace_back(new DeviceBuffer);
+      stage_bytes.push_back(0);
+    }
+    for (int i = 0; i < slots; ++i) workers.emplace_back([this, i] { worker(i); });
   }
 
   ~Server() {
@@ -203,7 +212,7 @@ struct Server {
   // Under the lock: the resources job j would take, or false if they do
   // not fit now.  On success they are marked in use (new ones are created
   // by the worker outside the lock) and accounted.
-  bool try_admit(Job *j) {
+  bool try_admit(Job *j, int slot) {
     const fc_job &s = j->spec;
     const int ngrids = s.kind == FC_SURVEY ? 2 : 1;
     const std::string gk = grid_key(s), ck = corr_key(s);
@@ -229,8 +238,10 @@ struct Server {
     if (!corr)
       extra += correlator_footprint(s.kind, s.shape, s.cell, s.rmax, s.kmax,
                                     s.maxell, s.precision);
-    const size_t transient = (size_t)need_n * 32;
-    extra += transient;
+    // The worker's staging grows to the largest catalog it has seen.
+    const size_t need_stage = (size_t)need_n * 32;
+    const size_t grow_stage = need_stage > stage_bytes[slot] ? need_stage - stage_bytes[slot] : 0;
+    extra += grow_stage;
     // Idle residents not reused here can be evicted.
     size_t evictable = 0;
     for (auto &r : resident)
@@ -284,18 +295,21 @@ struct Server {
       j->held.push_back(r.get());
       resident.push_back(std::move(r));
     }
-    j->transient = transient;
-    bytes_transient += transient;
+    if (grow_stage) {
+      stage_bytes[slot] += grow_stage;
+      bytes_resident += grow_stage;
+    }
+    j->transient = 0;
     peak_bytes = std::max(peak_bytes, used_bytes());
     return true;
   }
 
   size_t used_bytes() const { return bytes_resident + bytes_transient; }
 
-  Job *next_job() {
+  Job *next_job(int slot) {
     for (size_t i = 0; i < queue.size(); ++i) {
       Job *j = queue[i];
-      if (try_admit(j)) {
+      if (try_admit(j, slot)) {
         queue.erase(queue.begin() + i);
         if (i > 0) ++admitted_out_of_order;
         for (size_t k = 0; k < i; ++k) ++queue[k]->bypassed;
@@ -308,7 +322,7 @@ struct Server {
   }
 
   // ---------------------------------------------------------------- work
-  void worker() {
+  void worker(int slot) {
     cudaSetDevice(device);
     for (;;) {
       Job *j = nullptr;
@@ -316,7 +330,7 @@ struct Server {
         std::unique_lock<std::mutex> g(mu);
         // Admissible jobs are drained before a stop takes effect.
         cv_work.wait(g, [&] {
-          j = next_job();
+          j = next_job(slot);
           return j != nullptr || (stopping && queue.empty());
         });
         if (!j) return;
@@ -326,7 +340,7 @@ struct Server {
         peak_running = std::max(peak_running, running);
       }
       try {
-        run(j);
+        run(j, slot);
       } catch (const Error &e) {
         j->status = e.code;
         j->message = e.what();
@@ -376,8 +390,14 @@ struct Server {
                        &t.zerolag);
   }
 
-  void run(Job *j) {
+  void run(Job *j, int slot) {
     const fc_job &s = j->spec;
+    double t = now_s();
+    auto lap = [&](int k) {
+      const double t1 = now_s();
+      j->phase[k] += t1 - t;
+      t = t1;
+    };
     const std::string gk = grid_key(s);
     std::vector<Resident *> grids;
     Resident *cr = nullptr;
@@ -401,33 +421,29 @@ struct Server {
                                 s.precision);
     Grid *ga = grids[0]->grid.get();
     const int64_t nmax = max_particles(s);
-    double *stage = nullptr;
+    stage[slot]->resize(std::max<size_t>((size_t)nmax * 32, 32));
+    double *buf = stage[slot]->as<double>();
     cudaStream_t st = ga->stream;
-    if (nmax > 0) FC_CUDA(cudaMallocAsync(&stage, (size_t)nmax * 32, st));
-    struct Free {
-      double *p;
-      cudaStream_t s;
-      ~Free() {
-        if (p) {
-          cudaFreeAsync(p, s);
-          cudaStreamSynchronize(s);
-        }
-      }
-    } free_stage{stage, st};
+    lap(7);
     // Data grid.
     ga->clear();
     assignor_clear(grids[0]->ma);
-    catalog_generate(s.data, stage, st);
-    assignor_add_device(grids[0]->ma, stage, s.data.n);
+    catalog_generate(s.data, buf, st);
+    FC_CUDA(cudaStreamSynchronize(st));
+    lap(0);
+    assignor_add_device(grids[0]->ma, buf, s.data.n);
     assignor_stats(grids[0]->ma, &j->data_stats);
+    lap(1);
     fc_grid *ha = reinterpret_cast<fc_grid *>(ga);
     if (s.kind == FC_PERIODIC) {
       // cc/fftcorr.cc:369-375.
       const double mean = j->data_stats.totw / (double)ga->size();
       check(fc_grid_add_scalar(ha, -mean));
       check(fc_grid_multiply_by(ha, 1.0 / mean));
+      lap(4);
       correlator_autocorrelate(cr->corr, ga);
       read_tables(cr->corr, j, j->nn);
+      lap(5);
       return;
     }
     // Survey: randoms into the second grid, scaled by -alpha.
@@ -435,23 +451,28 @@ struct Server {
     gb->clear();
     assignor_clear(grids[1]->ma);
     stream_after(gb->stream, st);
-    catalog_generate(s.randoms, stage, gb->stream);
-    assignor_add_device(grids[1]->ma, stage, s.randoms.n);
+    catalog_generate(s.randoms, buf, gb->stream);
+    FC_CUDA(cudaStreamSynchronize(gb->stream));
+    lap(2);
+    assignor_add_device(grids[1]->ma, buf, s.randoms.n);
     assignor_stats(grids[1]->ma, &j->rand_stats);
+    lap(3);
     fc_grid *hb = reinterpret_cast<fc_grid *>(gb);
     FC_REQUIRE(j->rand_stats.totw != 0.0, FC_ERR_INVALID,
                "randoms have zero total weight");
     const double alpha = j->data_stats.totw / j->rand_stats.totw;
     check(fc_grid_multiply_by(hb, -alpha));
     check(fc_grid_axpy(ha, 1.0, hb));
+    lap(4);
     correlator_autocorrelate(cr->corr, ga);
     read_tables(cr->corr, j, j->nn);
+    lap(5);
     if (s.want_rr) {
       correlator_autocorrelate(cr->corr, gb);
       read_tables(cr->corr, j, j->rr);
       j->has_rr = true;
     }
-    stream_after(st, gb->stream);
+    lap(6);
   }
 
   static void check(int rc) {
@@ -554,6 +575,7 @@ int fc_server_job_info(fc_server *server, uint64_t ticket, fc_job_info *info) {
     info->nr = j->nr;
     info->nk = j->nk;
     info->has_rr = j->has_rr ? 1 : 0;
+    for (int k = 0; k < 8; ++k) info->phase_s[k] = j->phase[k];
     info->data = j->data_stats;
     info->randoms = j->rand_stats;
     std::strncpy(info->message, j->message.c_str(), sizeof(info->message) - 1);

@@ -130,7 +130,10 @@ class Server:
         i = _lib.JobInfo()
         _lib.call("fc_server_job_info", self._handle, int(ticket), ctypes.byref(i))
         out = {name: getattr(i, name) for name, _ in i._fields_
-               if name not in ("data", "randoms", "message")}
+               if name not in ("data", "randoms", "message", "phase_s")}
+        out["phase_s"] = dict(zip(("data_catalog", "data_assign", "random_catalog",
+                                   "random_assign", "combine", "correlate_nn",
+                                   "correlate_rr", "build"), list(i.phase_s)))
         out["message"] = i.message.decode("utf-8", "replace")
         out["data_totw"] = i.data.totw
         out["data_added"] = i.data.num_added

@@ -310,6 +310,11 @@ typedef struct fc_job_info {
   size_t footprint;         /* admission estimate, bytes                   */
   int nrows, nr, nk, has_rr;
   fc_assign_stats data, randoms;
+  double phase_s[8];        /* host time per phase: data catalog, data
+                               assignment, random catalog, random
+                               assignment, combine / normalise, NN
+                               correlate, RR correlate, building resident
+                               objects                                     */
   char message[256];        /* error message of a failed job               */
 } fc_job_info;
 typedef struct fc_server_stats {
@@ -458,6 +463,8 @@ int fc_device_malloc(size_t bytes, void **ptr);
 int fc_device_free(void *ptr);
 int fc_memcpy_htod(void *dst, const void *src, size_t bytes);
 int fc_memcpy_dtoh(void *dst, const void *src, size_t bytes);
+/* Free and total device memory (cudaMemGetInfo). */
+int fc_device_memory(size_t *free_bytes, size_t *total_bytes);
 /* Device-timeline stopwatch: start and stop synchronise the device and
  * record an event on the default stream, so the interval covers all work
  * issued in between on any stream. */
