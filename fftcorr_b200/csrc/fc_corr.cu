@@ -1013,6 +1013,8 @@ size_t correlator_footprint(int kind, const int shape[3], double cell,
     bytes += (size_t)g.rsize * g.shape[1] * h * eb;          // Wr
     bytes += (size_t)g.rsize * g.rsize * h * eb;             // Wry
     if (precision != FC_FP64) bytes += g.ncells() * 4;       // FP32 density
+    const int nlm = maxell == 0 ? 1 : maxell == 2 ? 6 : 15;
+    bytes += (size_t)nlm * g.kcells() * 8;                   // k weights
   } else {
     bytes += g.nreal_padded() * rb;                          // work
     if (kind == FC_SURVEY) bytes += g.ncomplex() * eb;       // grid2 FFT

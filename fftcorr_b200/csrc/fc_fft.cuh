@@ -26,6 +26,62 @@ struct Vec2<double> {
   using type = double2;
 };
 
+// Arithmetic on float2 as a vector of two lanes (used by CPair below).
+__device__ __forceinline__ float2 operator+(float2 a, float2 b) {
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ float2 operator-(float2 a, float2 b) {
+  return make_float2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ float2 operator-(float2 a) {
+  return make_float2(-a.x, -a.y);
+}
+__device__ __forceinline__ float2 operator*(float2 a, float s) {
+  return make_float2(a.x * s, a.y * s);
+}
+__device__ __forceinline__ float2 operator*(float s, float2 a) {
+  return make_float2(s * a.x, s * a.y);
+}
+__device__ __forceinline__ float2 operator*(float2 a, float2 b) {
+  return make_float2(a.x * b.x, a.y * b.y);  // lane by lane
+}
+
+// Two complex numbers of two independent transforms (columns or rows)
+// carried through one FFT together: x holds both real parts, y both
+// imaginary parts.  Twiddles are shared, shared-memory exchanges move 16
+// bytes at a time.
+struct __align__(16) CPair {
+  float2 x, y;
+};
+__device__ __forceinline__ CPair cpack(float2 a, float2 b) {
+  CPair r;
+  r.x = make_float2(a.x, b.x);
+  r.y = make_float2(a.y, b.y);
+  return r;
+}
+__device__ __forceinline__ float2 clane0(const CPair &v) {
+  return make_float2(v.x.x, v.y.x);
+}
+__device__ __forceinline__ float2 clane1(const CPair &v) {
+  return make_float2(v.x.y, v.y.y);
+}
+
+// Scalar type of a complex (or complex-pair) type.
+template <typename C>
+struct Real;
+template <>
+struct Real<float2> {
+  using type = float;
+};
+template <>
+struct Real<double2> {
+  using type = double;
+};
+template <>
+struct Real<CPair> {
+  using type = float;
+};
+
 template <typename C>
 __device__ __forceinline__ C cadd(C a, C b) {
   C r;
@@ -62,12 +118,24 @@ __device__ __forceinline__ C cconj(C a) {
   r.y = -a.y;
   return r;
 }
+// A pair times one shared complex twiddle.
+__device__ __forceinline__ CPair cmul(CPair a, float2 w) {
+  CPair r;
+  r.x = a.x * w.x - a.y * w.y;
+  r.y = a.x * w.y + a.y * w.x;
+  return r;
+}
 // (sign * i) * a
 template <typename C>
 __device__ __forceinline__ C cmuli(C a, int sign) {
   C r;
-  r.x = -sign * a.y;
-  r.y = sign * a.x;
+  if (sign > 0) {
+    r.x = -a.y;
+    r.y = a.x;
+  } else {
+    r.x = a.y;
+    r.y = -a.x;
+  }
   return r;
 }
 template <typename C, typename T>
@@ -109,8 +177,9 @@ template <typename C>
 struct Dft<8, C> {
   // Radix 2 across stride 4, then two radix-4 DFTs (even and odd outputs).
   __device__ static void run(C *v, int sign) {
-    using T = decltype(v[0].x);
+    using T = typename Real<C>::type;
     const T h = (T)0.70710678118654752440;
+    const T sg = (T)sign;
     C a[4], b[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -120,12 +189,12 @@ struct Dft<8, C> {
     // b[u] *= e^{sign 2 pi i u / 8}
     {
       C t = b[1];
-      b[1].x = h * (t.x - sign * t.y);
-      b[1].y = h * (t.y + sign * t.x);
+      b[1].x = h * (t.x - sg * t.y);
+      b[1].y = h * (t.y + sg * t.x);
       b[2] = cmuli(b[2], sign);
       t = b[3];
-      b[3].x = h * (-t.x - sign * t.y);
-      b[3].y = h * (-t.y + sign * t.x);
+      b[3].x = h * (-t.x - sg * t.y);
+      b[3].y = h * (-t.y + sg * t.x);
     }
     Dft<4, C>::run(a, sign);
     Dft<4, C>::run(b, sign);
@@ -292,22 +361,22 @@ namespace fc {
 // w^2 and w^4 come from the order-L root table and the rest are products.
 // ---------------------------------------------------------------------------
 
-template <typename C>
-__device__ __forceinline__ C tw_load(const C *__restrict__ tab, int idx,
-                                     int sign) {
-  C w = __ldg(&tab[idx]);
+template <typename Tw>
+__device__ __forceinline__ Tw tw_load(const Tw *__restrict__ tab, int idx,
+                                      int sign) {
+  Tw w = __ldg(&tab[idx]);
   if (sign > 0) w.y = -w.y;
   return w;
 }
 
 // One radix-8 pass with Ns > 1 for butterfly j = t on registers v.
-template <typename C>
+template <typename C, typename Tw>
 __device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
-                                           const C *__restrict__ tab, int sign) {
-  const C w1 = tw_load(tab, k * step, sign);
-  const C w2 = tw_load(tab, 2 * k * step, sign);
-  const C w4 = tw_load(tab, 4 * k * step, sign);
-  const C w3 = cmul(w1, w2);
+                                           const Tw *__restrict__ tab, int sign) {
+  const Tw w1 = tw_load(tab, k * step, sign);
+  const Tw w2 = tw_load(tab, 2 * k * step, sign);
+  const Tw w4 = tw_load(tab, 4 * k * step, sign);
+  const Tw w3 = cmul(w1, w2);
   v[1] = cmul(v[1], w1);
   v[2] = cmul(v[2], w2);
   v[3] = cmul(v[3], w3);
@@ -320,9 +389,9 @@ __device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
 // Transform of one column held in registers (layout above).  ex(i) gives the
 // shared-memory slot of row i of this thread's column; all TPC threads of
 // every column in the CTA must call this together.
-template <int L, typename C, typename Ex>
+template <int L, typename C, typename Tw, typename Ex>
 __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
-                                        const C *__restrict__ tab, int sign,
+                                        const Tw *__restrict__ tab, int sign,
                                         int tab_scale = 1) {
   constexpr int TPC = L / 8;
   // Number of radix-8 passes and the leading radix (1, 2 or 4).

@@ -20,6 +20,7 @@
 // separate make_ylm / cuFFT r2c / multiply / extract / cuFFT c2r passes.
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "fc_common.cuh"
@@ -235,10 +236,7 @@ template <typename T, int MODE>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     k_xcorr(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
             C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
-            const C2<T> *__restrict__ tabx, const double *__restrict__ kx,
-            const double *__restrict__ ky, const double *__restrict__ kz,
-            const double *__restrict__ wx, const double *__restrict__ wy,
-            const double *__restrict__ wz, YlmParams pk) {
+            const C2<T> *__restrict__ tabx, const double *__restrict__ ktab) {
   using C = C2<T>;
   constexpr int B = Tile<T>::B;
   constexpr int BP = B + 1;
@@ -290,10 +288,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
               const int x = refl == 0 ? ((i - ox) % g.n0 + g.n0) % g.n0
                                       : ((ox - i) % g.n0 + g.n0) % g.n0;
               const double re = (double)buf[x * BP + b].x;
-              const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
-              const double yv = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
-              double *dst = ksub + ((size_t)i * g.ks1 + j) * g.ks2 + k;
-              *dst += yv * re;
+              const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
+              ksub[cell] += ktab[cell] * re;
             }
           }
         }
@@ -405,6 +401,15 @@ struct P2 {
   static constexpr int TPC = L / 8;
   static constexpr int THREADS = TPC * B;
   static constexpr int BP = B + 1;
+  // Exchange rows of B elements: a 128-byte shared-memory line holds R of
+  // them.  Row i is stored at row i ^ ((i >> 3) & (R - 1)), which spreads
+  // the rows a warp touches in every Stockham write and read evenly over
+  // the line's R parts (bank-conflict free), with no padding.
+  static constexpr int RB = B * (int)sizeof(C2<T>);
+  static constexpr int R = RB >= 128 ? 1 : 128 / RB;
+  __device__ static __forceinline__ int row(int i) {
+    return i ^ ((i >> 3) & (R - 1));
+  }
 };
 
 template <typename T, int L>
@@ -427,7 +432,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
     v[u].y = 0;
     if (valid) v[u] = W[base + (int64_t)(t + Q::TPC * u) * g.h];
   }
-  reg_fft<L>(v, t, [&](int i) { return &ex[i * Q::BP + b]; }, taby, -1);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; }, taby, -1);
   if (valid) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) W[base + (int64_t)(t + Q::TPC * u) * g.h] = v[u];
@@ -455,7 +460,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
     v[u].y = 0;
     if (valid) v[u] = Wr[base + (int64_t)(t + Q::TPC * u) * g.h];
   }
-  reg_fft<L>(v, t, [&](int i) { return &ex[i * Q::BP + b]; }, taby, +1);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; }, taby, +1);
   if (!valid) return;
   const int64_t obase = (int64_t)ri * g.rs * g.h + kz0 + b;
 #pragma unroll
@@ -470,10 +475,7 @@ template <typename T, int L, int MODE>
 __global__ void __launch_bounds__(P2<T, L>::THREADS)
     k_xcorr_p2(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
                C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
-               const C2<T> *__restrict__ tabx, const double *__restrict__ kx,
-               const double *__restrict__ ky, const double *__restrict__ kz,
-               const double *__restrict__ wx, const double *__restrict__ wy,
-               const double *__restrict__ wz, YlmParams pk) {
+               const C2<T> *__restrict__ tabx, const double *__restrict__ ktab) {
   using C = C2<T>;
   using Q = P2<T, L>;
   extern __shared__ unsigned char smem_raw[];
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const bool valid = kzi < g.h;
   const int64_t stride = (int64_t)g.n1 * g.h;
   const int64_t base = (int64_t)yy * g.h + kzi;
-  auto exf = [&](int i) { return &ex[i * Q::BP + b]; };
+  auto exf = [&](int i) { return &ex[Q::row(i) * Q::B + b]; };
   C v[8];
   // In product mode the G column is loaded together with the W column, so
   // both streams are in flight during the forward transform.
@@ -530,10 +532,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
               const int x = refl == 0 ? ((i - ox) % L + L) % L
                                       : ((ox - i) % L + L) % L;
               const double re = (double)exf(x)->x;
-              const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
-              const double yv = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
-              double *dst = ksub + ((size_t)i * g.ks1 + j) * g.ks2 + k;
-              *dst += yv * re;
+              const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
+              ksub[cell] += ktab[cell] * re;
             }
           }
         }
@@ -682,6 +682,176 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   }
 }
 
+// ------------------------------------------------- FP32 two-per-thread
+// FP32 y and z passes with two independent transforms per thread (CPair):
+// the same B columns (or rows) per CTA as the kernels above with half the
+// threads.  The two transforms share every twiddle load and index
+// computation and the shared-memory exchanges move 16 bytes per access.
+// Thread (t, p) holds columns p and p + PB of the CTA's B, so each global
+// access of a warp stays contiguous per row.  (The x pass keeps one column
+// per thread: with its second input stream and inverse transform, two
+// columns per thread cost it more in occupancy than they save.)
+template <int L>
+struct PP {
+  static constexpr int B = P2<float, L>::B;
+  static constexpr int PB = B / 2;
+  static constexpr int TPC = L / 8;
+  static constexpr int THREADS = TPC * PB;
+  static constexpr int RB = PB * (int)sizeof(CPair);
+  static constexpr int R = RB >= 128 ? 1 : 128 / RB;
+  __device__ static __forceinline__ int row(int i) {
+    return i ^ ((i >> 3) & (R - 1));
+  }
+};
+
+template <int L>
+__global__ void __launch_bounds__(PP<L>::THREADS)
+    k_yfwd_pp(float2 *__restrict__ W, FusedGeom g,
+              const float2 *__restrict__ taby) {
+  using Q = PP<L>;
+  extern __shared__ unsigned char smem_raw[];
+  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  const int t = threadIdx.x / Q::PB;
+  const int p = threadIdx.x - t * Q::PB;
+  const int c0 = blockIdx.x * Q::B + p, c1 = c0 + Q::PB;
+  const bool v0 = c0 < g.h, v1 = c1 < g.h;
+  const int64_t base = (int64_t)blockIdx.y * L * g.h;
+  const float2 zero = make_float2(0.f, 0.f);
+  CPair v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
+    v[u] = cpack(v0 ? W[r + c0] : zero, v1 ? W[r + c1] : zero);
+  }
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; }, taby, -1);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
+    if (v0) W[r + c0] = clane0(v[u]);
+    if (v1) W[r + c1] = clane1(v[u]);
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(PP<L>::THREADS)
+    k_yinv_pp(const float2 *__restrict__ Wr, float2 *__restrict__ Wry,
+              FusedGeom g, const float2 *__restrict__ taby) {
+  using Q = PP<L>;
+  extern __shared__ unsigned char smem_raw[];
+  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  const int t = threadIdx.x / Q::PB;
+  const int p = threadIdx.x - t * Q::PB;
+  const int c0 = blockIdx.x * Q::B + p, c1 = c0 + Q::PB;
+  const bool v0 = c0 < g.h, v1 = c1 < g.h;
+  const int ri = blockIdx.y;
+  const int64_t base = (int64_t)ri * L * g.h;
+  const float2 zero = make_float2(0.f, 0.f);
+  CPair v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
+    v[u] = cpack(v0 ? Wr[r + c0] : zero, v1 ? Wr[r + c1] : zero);
+  }
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; }, taby, +1);
+  const int64_t obase = (int64_t)ri * g.rs * g.h;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int y = t + Q::TPC * u;
+    for (int rj = (y + g.ro) % L; rj < g.rs; rj += L) {
+      if (v0) Wry[obase + (int64_t)rj * g.h + c0] = clane0(v[u]);
+      if (v1) Wry[obase + (int64_t)rj * g.h + c1] = clane1(v[u]);
+    }
+  }
+}
+
+// Rows of the z transform, two rows per thread: rows b and b + PB of the
+// CTA's B, thread t of a row pair holding z[t + TPC u] of both.
+template <int L, bool WEIGHT>
+__global__ void __launch_bounds__(PP<L>::THREADS)
+    k_zfwd_pp(const float *__restrict__ rho, float2 *__restrict__ W, FusedGeom g,
+              YlmParams p, double x0, double y0, double z0,
+              const float2 *__restrict__ tabz) {
+  using Q = PP<L>;
+  constexpr int RP = L + L / 8 + 1;
+  extern __shared__ unsigned char smem_raw[];
+  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  const int pb = threadIdx.x / Q::TPC;
+  const int t = threadIdx.x - pb * Q::TPC;
+  const int64_t nrows = (int64_t)g.n0 * g.n1;
+  const int64_t row0 = (int64_t)blockIdx.x * Q::B + pb;
+  const int64_t row1 = row0 + Q::PB;
+  const bool v0 = row0 < nrows, v1 = row1 < nrows;
+  const float2 *src0 = reinterpret_cast<const float2 *>(rho + (v0 ? row0 : 0) * g.n2);
+  const float2 *src1 = reinterpret_cast<const float2 *>(rho + (v1 ? row1 : 0) * g.n2);
+  RowPoly rp0, rp1;
+  float zt = 0.f;
+  if constexpr (WEIGHT) {
+    const int xa = (int)(row0 / g.n1), ya = (int)(row0 - (int64_t)xa * g.n1);
+    const int xb = (int)(row1 / g.n1), yb = (int)(row1 - (int64_t)xb * g.n1);
+    rp0 = row_poly(p, x0 + xa * 1.0, y0 + ya * 1.0);
+    rp1 = row_poly(p, x0 + xb * 1.0, y0 + yb * 1.0);
+    zt = (float)(z0 + (2 * t) * 1.0);
+  }
+  const float2 zero = make_float2(0.f, 0.f);
+  CPair v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int jj = t + Q::TPC * u;
+    float2 a = v0 ? src0[jj] : zero;
+    float2 b = v1 ? src1[jj] : zero;
+    if constexpr (WEIGHT) {
+      const float zu = zt + (float)(2 * Q::TPC * u);
+      a.x = row_weight(rp0, a.x, zu);
+      a.y = row_weight(rp0, a.y, zu + 1.0f);
+      b.x = row_weight(rp1, b.x, zu);
+      b.y = row_weight(rp1, b.y, zu + 1.0f);
+    }
+    v[u] = cpack(a, b);
+  }
+  auto exf = [&](int i) { return &ex[pb * RP + i + (i >> 3)]; };
+  reg_fft<L>(v, t, exf, tabz, -1, 2);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
+  __syncthreads();
+  float2 *dst0 = W + row0 * g.h;
+  float2 *dst1 = W + row1 * g.h;
+  for (int k = t; k <= L; k += Q::TPC) {
+    const CPair a = *exf(k == L ? 0 : k);
+    const CPair c = cconj(*exf(k == 0 ? 0 : L - k));
+    CPair e, o;
+    e.x = 0.5f * (a.x + c.x);
+    e.y = 0.5f * (a.y + c.y);
+    const CPair d = csub(a, c);
+    o.x = 0.5f * d.y;
+    o.y = -0.5f * d.x;
+    const CPair r = cadd(e, cmul(o, __ldg(&tabz[k])));
+    if (v0) dst0[k] = clane0(r);
+    if (v1) dst1[k] = clane1(r);
+  }
+}
+
+// Per-cell k-subgrid weight of one (ell, m): Y_lm(k) * 4 pi / (W(kx) W(ky)
+// W(kz)) with make_ylm's arithmetic (correlator.h:453-466), computed once
+// per correlator and multipole so the extraction in the x pass is a
+// multiply-add.
+__global__ void k_ktable(double *__restrict__ tab, int k0, int k1, int k2,
+                         const double *__restrict__ kx,
+                         const double *__restrict__ ky,
+                         const double *__restrict__ kz,
+                         const double *__restrict__ wx,
+                         const double *__restrict__ wy,
+                         const double *__restrict__ wz, YlmParams pk) {
+  const size_t n = (size_t)k0 * k1 * k2;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n;
+       c += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(c % k2);
+    const int j = (int)((c / k2) % k1);
+    const int i = (int)(c / ((size_t)k2 * k1));
+    const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
+    tab[c] = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
+  }
+}
+
 __global__ void k_to_float(const double *__restrict__ in, float *__restrict__ out,
                            size_t n, double shift) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -740,7 +910,7 @@ bool is_p2(int L) { return L >= 64 && L <= 2048 && (L & (L - 1)) == 0; }
 
 template <typename T, int L>
 size_t p2_col_smem() {
-  return (size_t)L * P2<T, L>::BP * sizeof(C2<T>);
+  return (size_t)L * P2<T, L>::B * sizeof(C2<T>);
 }
 template <typename T, int L>
 size_t p2_row_smem() {
@@ -777,6 +947,16 @@ void p2_set_limits() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   FC_CUDA(cudaFuncSetAttribute(k_zinv_p2<T, L>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  if constexpr (std::is_same_v<T, float>) {
+    FC_CUDA(cudaFuncSetAttribute(k_yfwd_pp<L>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_yinv_pp<L>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  }
 }
 
 }  // namespace
@@ -892,6 +1072,18 @@ void FusedSurvey::zfwd(const void *rho, bool weight, const YlmParams &p,
       using Q = P2<T, L>;
       const int64_t nrows = (int64_t)g.n0 * g.n1;
       const unsigned blocks = (unsigned)((nrows + Q::B - 1) / Q::B);
+      if constexpr (std::is_same_v<T, float>) {
+        using PQ = PP<L>;
+        if (weight)
+          k_zfwd_pp<L, true><<<blocks, PQ::THREADS, p2_row_smem<T, L>(), s>>>(
+              (const float *)rho, W.as<float2>(), g, p, xyz0[0], xyz0[1],
+              xyz0[2], tabz.as<float2>());
+        else
+          k_zfwd_pp<L, false><<<blocks, PQ::THREADS, p2_row_smem<T, L>(), s>>>(
+              (const float *)rho, W.as<float2>(), g, p, xyz0[0], xyz0[1],
+              xyz0[2], tabz.as<float2>());
+        return;
+      }
       if (weight)
         k_zfwd_p2<T, L, true><<<blocks, Q::THREADS, p2_row_smem<T, L>(), s>>>(
             (const T *)rho, W.as<C2<T>>(), g, p, xyz0[0], xyz0[1], xyz0[2],
@@ -926,8 +1118,12 @@ void FusedSurvey::yfwd(cudaStream_t s) {
     with_p2(g.n1, [&]<int L>() {
       using Q = P2<T, L>;
       dim3 grid((g.h + Q::B - 1) / Q::B, g.n0);
-      k_yfwd_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
-          W.as<C2<T>>(), g, taby.as<C2<T>>());
+      if constexpr (std::is_same_v<T, float>)
+        k_yfwd_pp<L><<<grid, PP<L>::THREADS, p2_col_smem<T, L>(), s>>>(
+            W.as<float2>(), g, taby.as<float2>());
+      else
+        k_yfwd_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+            W.as<C2<T>>(), g, taby.as<C2<T>>());
     });
     FC_LAUNCH_CHECK();
     return;
@@ -940,8 +1136,8 @@ void FusedSurvey::yfwd(cudaStream_t s) {
 }
 
 template <typename T>
-void FusedSurvey::xcorr(bool product, double *ksub, const KAxes &ka,
-                        const YlmParams &pk, cudaStream_t s) {
+void FusedSurvey::xcorr(bool product, double *ksub, const double *ktab,
+                        cudaStream_t s) {
   if (is_p2(g.n0)) {
     with_p2(g.n0, [&]<int L>() {
       using Q = P2<T, L>;
@@ -949,11 +1145,11 @@ void FusedSurvey::xcorr(bool product, double *ksub, const KAxes &ka,
       if (!product)
         k_xcorr_p2<T, L, 0><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
-            ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
+            nullptr);
       else
         k_xcorr_p2<T, L, 1><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g,
-            tabx.as<C2<T>>(), ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
+            tabx.as<C2<T>>(), ktab);
     });
     FC_LAUNCH_CHECK();
     return;
@@ -965,11 +1161,11 @@ void FusedSurvey::xcorr(bool product, double *ksub, const KAxes &ka,
   if (!product) {
     k_xcorr<T, 0><<<grid, threads, sm, s>>>(
         W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
-        ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
+        nullptr);
   } else {
     k_xcorr<T, 1><<<grid, threads, sm, s>>>(
         W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g, tabx.as<C2<T>>(),
-        ka.kx, ka.ky, ka.kz, ka.wx, ka.wy, ka.wz, pk);
+        ktab);
   }
   FC_LAUNCH_CHECK();
 }
@@ -980,8 +1176,12 @@ void FusedSurvey::yinv(cudaStream_t s) {
     with_p2(g.n1, [&]<int L>() {
       using Q = P2<T, L>;
       dim3 grid((g.h + Q::B - 1) / Q::B, g.rs);
-      k_yinv_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
-          Wr.as<C2<T>>(), Wry.as<C2<T>>(), g, taby.as<C2<T>>());
+      if constexpr (std::is_same_v<T, float>)
+        k_yinv_pp<L><<<grid, PP<L>::THREADS, p2_col_smem<T, L>(), s>>>(
+            Wr.as<float2>(), Wry.as<float2>(), g, taby.as<float2>());
+      else
+        k_yinv_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+            Wr.as<C2<T>>(), Wry.as<C2<T>>(), g, taby.as<C2<T>>());
     });
     FC_LAUNCH_CHECK();
     return;
@@ -1015,17 +1215,33 @@ void FusedSurvey::zinv(double *rsub, const double *raxis, const YlmParams &pr,
   FC_LAUNCH_CHECK();
 }
 
+const double *FusedSurvey::k_table(int ell, int m, const KAxes &ka,
+                                   cudaStream_t s) {
+  const int key = ell * 16 + (m + ell);
+  auto it = ktabs.find(key);
+  if (it != ktabs.end()) return it->second.as<double>();
+  const size_t n = (size_t)g.ks0 * g.ks1 * g.ks2;
+  DeviceBuffer &b = ktabs[key];
+  b.resize(std::max<size_t>(n, 1) * sizeof(double));
+  k_ktable<<<grid_for(n, 256), 256, 0, s>>>(
+      b.as<double>(), g.ks0, g.ks1, g.ks2, ka.kx, ka.ky, ka.kz, ka.wx, ka.wy,
+      ka.wz, make_ylm_params(ell, m, 4.0 * M_PI));
+  FC_LAUNCH_CHECK();
+  return b.as<double>();
+}
+
 void FusedSurvey::grid2(const void *rho_in, cudaStream_t s, const KAxes &ka) {
+  (void)ka;
   YlmParams none = make_ylm_params(0, 0, 1.0);
   const double zero[3] = {0, 0, 0};
   if (fp64_) {
     zfwd<double>(rho_in, false, none, zero, s);
     yfwd<double>(s);
-    xcorr<double>(false, nullptr, ka, none, s);
+    xcorr<double>(false, nullptr, nullptr, s);
   } else {
     zfwd<float>(rho_in, false, none, zero, s);
     yfwd<float>(s);
-    xcorr<float>(false, nullptr, ka, none, s);
+    xcorr<float>(false, nullptr, nullptr, s);
   }
 }
 
@@ -1034,8 +1250,8 @@ void FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
                        const double *raxis, const KAxes &ka, cudaStream_t s,
                        PhaseHook *hook) {
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
-  const YlmParams pk = make_ylm_params(ell, m, 4.0 * M_PI);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
+  const double *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
   auto run = [&](auto tag) {
     using T = decltype(tag);
     if (hook) hook->begin("zfwd");
@@ -1045,7 +1261,7 @@ void FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
     yfwd<T>(s);
     if (hook) hook->end();
     if (hook) hook->begin("xcorr");
-    xcorr<T>(true, ksub, ka, pk, s);
+    xcorr<T>(true, ksub, ktab, s);
     if (hook) hook->end();
     if (hook) hook->begin("yinv");
     yinv<T>(s);

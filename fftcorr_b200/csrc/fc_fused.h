@@ -2,6 +2,7 @@
 // (see fc_fused.cu for the algorithm).
 #pragma once
 
+#include <map>
 #include <vector>
 
 #include "fc_common.cuh"
@@ -67,8 +68,9 @@ class FusedSurvey {
   template <typename T>
   void yfwd(cudaStream_t s);
   template <typename T>
-  void xcorr(bool product, double *ksub, const KAxes &ka, const YlmParams &pk,
-             cudaStream_t s);
+  void xcorr(bool product, double *ksub, const double *ktab, cudaStream_t s);
+  // Weights of the k-subgrid cells for (ell, m), built on first use.
+  const double *k_table(int ell, int m, const KAxes &ka, cudaStream_t s);
   template <typename T>
   void yinv(cudaStream_t s);
   template <typename T>
@@ -78,6 +80,7 @@ class FusedSurvey {
   bool fp64_;
   DeviceBuffer tabx, taby, tabz;
   DeviceBuffer W, G, Wr, Wry, rho32;
+  std::map<int, DeviceBuffer> ktabs;
 };
 
 }  // namespace fc
