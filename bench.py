@@ -297,7 +297,9 @@ def kernel_profile(job, dD, nD, dR, nR):
 # --no-fp64 --no-cpu-baseline`; the pass kernels see the same grid as the
 # full workload (only the catalogs are smaller).  Summaries under profiles/.
 TRAFFIC_PER_LAUNCH_512 = {
-    "zfwd": 1028.45e6,
+    "zfwd": 1027.39e6,
+    "yfwd": 1024.73e6,
+    "xcorr": 1325.90e6,
 }
 
 
@@ -317,7 +319,7 @@ def algorithmic_bytes(family, w, precision, rs, ks):
       zfwd   density in (N * s) + W out (Nc * e)
       yfwd   W in and out (2 Nc e)
       xcorr  W and G in (2 Nc e) + x-pruned Wr out (rs N1 h e)
-             + k-subgrid read-modify-write (K0 K1 K2 * 16)
+             + k-subgrid weight read and read-modify-write (K0 K1 K2 * 24)
       yinv   Wr in (rs N1 h e) + Wry out (rs rs h e)
       zinv   Wry in (rs rs h e) + r-subgrid read-modify-write (rs^3 * 16)"""
     s = 8 if precision == "fp64" else 4
@@ -330,7 +332,7 @@ def algorithmic_bytes(family, w, precision, rs, ks):
     table = {
         "zfwd": n * s + nc * e,
         "yfwd": 2 * nc * e,
-        "xcorr": 2 * nc * e + rs * n1 * h * e + kc * 16,
+        "xcorr": 2 * nc * e + rs * n1 * h * e + kc * 24,
         "yinv": rs * n1 * h * e + rs * rs * h * e,
         "zinv": rs * rs * h * e + rs ** 3 * 16,
         "weight": n * 8 + n * s,
