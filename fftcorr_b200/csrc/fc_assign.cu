@@ -244,6 +244,18 @@ __global__ void k_tile_starts(const KeyT *keys, int64_t n, int64_t ntiles,
   }
 }
 
+// (tile, first particle, end) of every tile in colour order, so a scatter
+// CTA finds its work with one load.
+__global__ void k_tile_ranges(const uint32_t *__restrict__ tiles, int64_t nt,
+                              const uint32_t *__restrict__ tile_start,
+                              uint4 *__restrict__ ranges) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nt;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = tiles[i];
+    ranges[i] = make_uint4(t, tile_start[t], tile_start[t + 1], 0u);
+  }
+}
+
 // K-scatter for one colour pass.  Shared memory layout:
 //   acc[F^3] footprint sums | wts[kChunk][3W] | pcell[kChunk] | cstart[513]
 template <int S, typename KeyT>
@@ -392,8 +404,7 @@ template <int S, typename KeyT>
 __global__ void __launch_bounds__(kTileCells)
     k_scatter_s(const double *__restrict__ posw, const KeyT *__restrict__ keys,
                 const uint32_t *__restrict__ vals,
-                const uint32_t *__restrict__ tile_start,
-                const uint32_t *__restrict__ tiles, AssignGeom g,
+                const uint4 *__restrict__ ranges, AssignGeom g,
                 double *__restrict__ grid) {
   using Q = ScatterS<S>;
   constexpr int W = Q::W;
@@ -408,9 +419,10 @@ __global__ void __launch_bounds__(kTileCells)
   int *pc = reinterpret_cast<int *>(smem + 4 * C);     // [C], per chunk
   double *acc = smem + Q::region / 8;                  // [F3]
 
-  const uint32_t tile = tiles[blockIdx.x];
-  const uint32_t ts = tile_start[tile];
-  const uint32_t te = tile_start[tile + 1];
+  const uint4 rg = ranges[blockIdx.x];
+  const uint32_t tile = rg.x;
+  const uint32_t ts = rg.y;
+  const uint32_t te = rg.z;
   if (ts >= te) return;
   const int tz = tile % g.nt[2];
   const int ty = (tile / g.nt[2]) % g.nt[1];
@@ -418,6 +430,30 @@ __global__ void __launch_bounds__(kTileCells)
   const int o0 = tx * kTile, o1 = ty * kTile, o2 = tz * kTile;
   const int h = threadIdx.x;
   const KeyT kbase = (KeyT)tile * kTileCells;
+  // When no footprint wraps onto itself, each footprint cell has one
+  // global cell: load its current value now, so the latency of the final
+  // read-modify-write overlaps the particle gather.  (No other CTA of this
+  // colour pass touches these cells.)
+  constexpr int kFPer = (F3 + kTileCells - 1) / kTileCells;
+  const bool direct = g.n[0] >= F && g.n[1] >= F && g.n[2] >= F;
+  size_t gidx[kFPer];
+  double gval[kFPer];
+#pragma unroll
+  for (int r = 0; r < kFPer; ++r) {
+    const int f = threadIdx.x + r * kTileCells;
+    gidx[r] = 0;
+    gval[r] = 0.0;
+    if (direct && f < F3) {
+      int gx = (o0 + f / (F * F) + OMIN) % g.n[0];
+      int gy = (o1 + (f / F) % F + OMIN) % g.n[1];
+      int gz = (o2 + f % F + OMIN) % g.n[2];
+      if (gx < 0) gx += g.n[0];
+      if (gy < 0) gy += g.n[1];
+      if (gz < 0) gz += g.n[2];
+      gidx[r] = ((size_t)gx * g.n[1] + gy) * g.n[2] + gz;
+      gval[r] = grid[gidx[r]];
+    }
+  }
 
   double sacc[W3];
 #pragma unroll
@@ -481,6 +517,16 @@ __global__ void __launch_bounds__(kTileCells)
     acc[f] = a;
   }
   __syncthreads();
+  if (direct) {
+#pragma unroll
+    for (int r = 0; r < kFPer; ++r) {
+      const int f = threadIdx.x + r * kTileCells;
+      if (f >= F3) continue;
+      const double v = 0.0 + acc[f];
+      if (v != 0.0) grid[gidx[r]] = gval[r] + v;
+    }
+    return;
+  }
   // Each global cell is written by one footprint cell (its smallest alias
   // when the footprint wraps onto itself on grids narrower than F).
   for (int f = threadIdx.x; f < F3; f += blockDim.x) {
@@ -583,6 +629,7 @@ struct Assignor {
   DeviceBuffer posw, keys, keys_alt, vals, vals_alt, cub_temp;
   DeviceBuffer tile_start;
   DeviceBuffer color_tiles;
+  DeviceBuffer tile_ranges;            // uint4 per tile, colour order
   std::vector<int64_t> color_offsets;  // per colour, into color_tiles
   DeviceBuffer partials;               // K-key block partials
   DeviceBuffer totals;                 // [totw, totwsq]
@@ -620,6 +667,7 @@ struct Assignor {
     end_bit = 1;
     while (end_bit < 64 && (max_key >> end_bit) != 0) ++end_bit;
     tile_start.resize((ntiles + 1) * sizeof(uint32_t));
+    tile_ranges.resize(std::max<int64_t>(ntiles, 1) * sizeof(uint4));
     partials.resize(2 * kSumBlocks * sizeof(double));
     totals.resize(2 * sizeof(double));
     counts.resize(sizeof(unsigned long long));
@@ -860,21 +908,25 @@ struct Assignor {
         sk, n, ntiles, tile_start.as<uint32_t>());
     FC_LAUNCH_CHECK();
     const uint32_t *tiles = color_tiles.as<uint32_t>();
+    if (scheme != 2) {
+      k_tile_ranges<<<grid_for(ntiles, 256), 256, 0, stream()>>>(
+          tiles, ntiles, tile_start.as<uint32_t>(), tile_ranges.as<uint4>());
+      FC_LAUNCH_CHECK();
+    }
     for (size_t c = 0; c + 1 < color_offsets.size(); ++c) {
       const int64_t nt = color_offsets[c + 1] - color_offsets[c];
       if (nt == 0) continue;
       const uint32_t *ct = tiles + color_offsets[c];
+      const uint4 *cr = tile_ranges.as<uint4>() + color_offsets[c];
       switch (scheme) {
         case 0:
           k_scatter_s<0, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<0>(),
-                                 stream()>>>(src_posw, sk, sv,
-                                             tile_start.as<uint32_t>(), ct, geom,
+                                 stream()>>>(src_posw, sk, sv, cr, geom,
                                              grid->ptr());
           break;
         case 1:
           k_scatter_s<1, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<1>(),
-                                 stream()>>>(src_posw, sk, sv,
-                                             tile_start.as<uint32_t>(), ct, geom,
+                                 stream()>>>(src_posw, sk, sv, cr, geom,
                                              grid->ptr());
           break;
         case 2:
@@ -885,8 +937,7 @@ struct Assignor {
           break;
         default:
           k_scatter_s<3, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<3>(),
-                                 stream()>>>(src_posw, sk, sv,
-                                             tile_start.as<uint32_t>(), ct, geom,
+                                 stream()>>>(src_posw, sk, sv, cr, geom,
                                              grid->ptr());
           break;
       }

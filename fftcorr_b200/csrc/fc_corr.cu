@@ -819,12 +819,15 @@ struct Correlator {
   // Correlator::correlate_internal (correlator.h:406-497).  The reference
   // first transforms grid1 and then overwrites the result (:412-417); that
   // transform has no effect on any output and is not repeated here.
+  // prepared: the fused passes' input already holds rho (set_grid2 of the
+  // same grid has just converted it).
   template <typename T>
-  void survey_run(const double *rho) {
+  void survey_run(const double *rho, bool prepared = false) {
     const size_t ncells = geo.ncells();
     const int maxell = 2 * (geo.nrows - 1);
     if (fused) {
-      const void *in = fused->prepare_input(rho, stream);
+      const void *in =
+          prepared ? fused->input(rho) : fused->prepare_input(rho, stream);
       ProfHook hook(&prof, stream);
       const KAxes ka = kaxes();
       for (int ell = 0; ell <= maxell; ell += 2) {
@@ -865,7 +868,7 @@ struct Correlator {
       if (!cross) set_grid2_dev<T>(rho);
       FC_REQUIRE(have_g2, FC_ERR_STATE,
                  "cross_correlate needs set_grid2 or set_grid2_fft first");
-      survey_run<T>(rho);
+      survey_run<T>(rho, !cross);
     }
   }
 

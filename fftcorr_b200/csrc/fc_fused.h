@@ -43,6 +43,11 @@ class FusedSurvey {
   // The grid in the arithmetic of the passes: rho itself in FP64, an FP32
   // copy in mixed precision.
   const void *prepare_input(const double *rho, cudaStream_t s);
+  // What prepare_input(rho) last returned -- valid only while that density
+  // is unchanged.
+  const void *input(const double *rho) const {
+    return fp64_ ? (const void *)rho : rho32.get();
+  }
   // G = 3-D DFT of the prepared grid (BaseCorrelator::set_grid2).
   void grid2(const void *rho_in, cudaStream_t s, const KAxes &ka);
   // One (ell, m) term of Correlator::correlate_internal, accumulated into
