@@ -1015,7 +1015,8 @@ size_t correlator_footprint(int kind, const int shape[3], double cell,
     bytes += 2 * g.ncomplex() * eb;                          // W, G
     bytes += (size_t)g.rsize * g.shape[1] * h * eb;          // Wr
     bytes += (size_t)g.rsize * g.rsize * h * eb;             // Wry
-    if (precision != FC_FP64) bytes += g.ncells() * 4;       // FP32 density
+    if (precision != FC_FP64)                                // FP32 density,
+      bytes += g.ncells() * 4 + (size_t)g.shape[0] * g.shape[1] * 32;  // row table
     const int nlm = maxell == 0 ? 1 : maxell == 2 ? 6 : 15;
     bytes += (size_t)nlm * g.kcells() * 8;                   // k weights
   } else {

@@ -116,6 +116,23 @@ __device__ __forceinline__ float row_weight(const RowPoly &r, float D,
   return r.ell == 2 ? D * poly * ir2 : D * poly * (ir2 * ir2);
 }
 
+__device__ __forceinline__ RowPoly load_row_poly(const float4 *__restrict__ tab,
+                                                 int64_t row,
+                                                 const YlmParams &p) {
+  const float4 a = __ldg(&tab[2 * row]);
+  const float4 b = __ldg(&tab[2 * row + 1]);
+  RowPoly r;
+  r.c[0] = a.x;
+  r.c[1] = a.y;
+  r.c[2] = a.z;
+  r.c[3] = a.w;
+  r.c[4] = b.x;
+  r.rxy2 = b.y;
+  r.ell = p.ell;
+  r.value0 = (float)p.value0;
+  return r;
+}
+
 // ------------------------------------------------------------------ zfwd
 // B rows of N2 reals per CTA: (optionally Y_lm-weighted) packed as
 // z_j = x_2j + i x_2j+1, length-M complex DFT, then the real-to-complex
@@ -770,7 +787,8 @@ template <int L, bool WEIGHT>
 __global__ void __launch_bounds__(PP<L>::THREADS)
     k_zfwd_pp(const float *__restrict__ rho, float2 *__restrict__ W, FusedGeom g,
               YlmParams p, double x0, double y0, double z0,
-              const float2 *__restrict__ tabz) {
+              const float2 *__restrict__ tabz,
+              const float4 *__restrict__ rowtab) {
   using Q = PP<L>;
   constexpr int RP = L + L / 8 + 1;
   extern __shared__ unsigned char smem_raw[];
@@ -786,10 +804,16 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   RowPoly rp0, rp1;
   float zt = 0.f;
   if constexpr (WEIGHT) {
-    const int xa = (int)(row0 / g.n1), ya = (int)(row0 - (int64_t)xa * g.n1);
-    const int xb = (int)(row1 / g.n1), yb = (int)(row1 - (int64_t)xb * g.n1);
-    rp0 = row_poly(p, x0 + xa * 1.0, y0 + ya * 1.0);
-    rp1 = row_poly(p, x0 + xb * 1.0, y0 + yb * 1.0);
+    if (rowtab != nullptr) {
+      // Per-row coefficients from k_rowpoly (the same FP64 evaluation).
+      rp0 = load_row_poly(rowtab, v0 ? row0 : 0, p);
+      rp1 = load_row_poly(rowtab, v1 ? row1 : 0, p);
+    } else {
+      const int xa = (int)(row0 / g.n1), ya = (int)(row0 - (int64_t)xa * g.n1);
+      const int xb = (int)(row1 / g.n1), yb = (int)(row1 - (int64_t)xb * g.n1);
+      rp0 = row_poly(p, x0 + xa * 1.0, y0 + ya * 1.0);
+      rp1 = row_poly(p, x0 + xb * 1.0, y0 + yb * 1.0);
+    }
     zt = (float)(z0 + (2 * t) * 1.0);
   }
   const float2 zero = make_float2(0.f, 0.f);
@@ -815,7 +839,11 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   __syncthreads();
   float2 *dst0 = W + row0 * g.h;
   float2 *dst1 = W + row1 * g.h;
-  for (int k = t; k <= L; k += Q::TPC) {
+  // Unrolled so the twiddle loads of all outputs issue together.
+#pragma unroll
+  for (int i = 0; i <= L / Q::TPC; ++i) {
+    const int k = t + Q::TPC * i;
+    if (k > L) break;
     const CPair a = *exf(k == L ? 0 : k);
     const CPair c = cconj(*exf(k == 0 ? 0 : L - k));
     CPair e, o;
@@ -827,6 +855,20 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
     const CPair r = cadd(e, cmul(o, __ldg(&tabz[k])));
     if (v0) dst0[k] = clane0(r);
     if (v1) dst1[k] = clane1(r);
+  }
+}
+
+// Per-row Horner coefficients of one (ell, m) (row_poly), two float4 per
+// row, so the z pass does no FP64 work per row.
+__global__ void k_rowpoly(float4 *__restrict__ tab, int64_t nrows, int n1,
+                          YlmParams p, double x0, double y0) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+       row < nrows; row += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(row / n1);
+    const int y = (int)(row - (int64_t)x * n1);
+    const RowPoly r = row_poly(p, x0 + x * 1.0, y0 + y * 1.0);
+    tab[2 * row] = make_float4(r.c[0], r.c[1], r.c[2], r.c[3]);
+    tab[2 * row + 1] = make_float4(r.c[4], r.rxy2, 0.f, 0.f);
   }
 }
 
@@ -1007,7 +1049,10 @@ FusedSurvey::FusedSurvey(const int shape[3], int rsize, const int kshape[3],
   G.resize(nc * eb);
   Wr.resize((size_t)g.rs * g.n1 * g.h * eb);
   Wry.resize((size_t)g.rs * g.rs * g.h * eb);
-  if (!fp64) rho32.resize((size_t)g.n0 * g.n1 * g.n2 * sizeof(float));
+  if (!fp64) {
+    rho32.resize((size_t)g.n0 * g.n1 * g.n2 * sizeof(float));
+    rowtab.resize((size_t)g.n0 * g.n1 * 2 * sizeof(float4));
+  }
   set_smem_limits();
 }
 
@@ -1074,14 +1119,22 @@ void FusedSurvey::zfwd(const void *rho, bool weight, const YlmParams &p,
       const unsigned blocks = (unsigned)((nrows + Q::B - 1) / Q::B);
       if constexpr (std::is_same_v<T, float>) {
         using PQ = PP<L>;
+        const float4 *rt = nullptr;
+        if (weight && p.ell != 0) {
+          rowtab.resize((size_t)nrows * 2 * sizeof(float4));
+          k_rowpoly<<<grid_for(nrows, 256), 256, 0, s>>>(
+              rowtab.as<float4>(), nrows, g.n1, p, xyz0[0], xyz0[1]);
+          FC_LAUNCH_CHECK();
+          rt = rowtab.as<float4>();
+        }
         if (weight)
           k_zfwd_pp<L, true><<<blocks, PQ::THREADS, p2_row_smem<T, L>(), s>>>(
               (const float *)rho, W.as<float2>(), g, p, xyz0[0], xyz0[1],
-              xyz0[2], tabz.as<float2>());
+              xyz0[2], tabz.as<float2>(), rt);
         else
           k_zfwd_pp<L, false><<<blocks, PQ::THREADS, p2_row_smem<T, L>(), s>>>(
               (const float *)rho, W.as<float2>(), g, p, xyz0[0], xyz0[1],
-              xyz0[2], tabz.as<float2>());
+              xyz0[2], tabz.as<float2>(), nullptr);
         return;
       }
       if (weight)

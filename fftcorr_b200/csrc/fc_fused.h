@@ -86,6 +86,7 @@ class FusedSurvey {
   DeviceBuffer tabx, taby, tabz;
   DeviceBuffer W, G, Wr, Wry, rho32;
   std::map<int, DeviceBuffer> ktabs;
+  DeviceBuffer rowtab;  // per-row z-pass weight coefficients (FP32 form)
 };
 
 }  // namespace fc
