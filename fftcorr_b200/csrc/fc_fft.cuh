@@ -389,8 +389,10 @@ __device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
 // Transform of one column held in registers (layout above).  ex(i) gives the
 // shared-memory slot of row i of this thread's column; all TPC threads of
 // every column in the CTA must call this together.
-template <int L, typename C, typename Tw, typename Ex>
-__device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
+// rd(u) must return ex(t + TPC * u): kernels pass one that adds constant
+// offsets to a per-thread base instead of recomputing the layout's index.
+template <int L, typename C, typename Tw, typename Ex, typename Rd>
+__device__ __forceinline__ void reg_fft(C *v, int t, Ex ex, Rd rd,
                                         const Tw *__restrict__ tab, int sign,
                                         int tab_scale = 1) {
   constexpr int TPC = L / 8;
@@ -416,7 +418,7 @@ __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
     }
     __syncthreads();
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = *ex(t + TPC * u);
+    for (int u = 0; u < 8; ++u) v[u] = *rd(u);
     __syncthreads();
     Ns = 2;
   } else if constexpr (R0 == 4) {
@@ -438,7 +440,7 @@ __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
     }
     __syncthreads();
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = *ex(t + TPC * u);
+    for (int u = 0; u < 8; ++u) v[u] = *rd(u);
     __syncthreads();
     Ns = 4;
   }
@@ -453,11 +455,19 @@ __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
       for (int q = 0; q < 8; ++q) *ex(o + q * Ns) = v[q];
       __syncthreads();
 #pragma unroll
-      for (int u = 0; u < 8; ++u) v[u] = *ex(t + TPC * u);
+      for (int u = 0; u < 8; ++u) v[u] = *rd(u);
       __syncthreads();
     }
     Ns *= 8;
   }
+}
+
+template <int L, typename C, typename Tw, typename Ex>
+__device__ __forceinline__ void reg_fft(C *v, int t, Ex ex,
+                                        const Tw *__restrict__ tab, int sign,
+                                        int tab_scale = 1) {
+  reg_fft<L>(v, t, ex, [&](int u) { return ex(t + (L / 8) * u); }, tab, sign,
+             tab_scale);
 }
 
 }  // namespace fc

@@ -427,6 +427,16 @@ struct P2 {
   __device__ static __forceinline__ int row(int i) {
     return i ^ ((i >> 3) & (R - 1));
   }
+  // Element index of row t + TPC u, column b: when TPC / 8 is a multiple
+  // of R the swizzle only depends on t, so it is a per-thread base plus u
+  // times a constant.
+  static constexpr bool kFastRead = (TPC / 8) % R == 0;
+  __device__ static __forceinline__ int rd_base(int t, int b) {
+    return kFastRead ? row(t) * B + b : 0;
+  }
+  __device__ static __forceinline__ int rd(int base, int t, int b, int u) {
+    return kFastRead ? base + u * TPC * B : row(t + TPC * u) * B + b;
+  }
 };
 
 template <typename T, int L>
@@ -449,7 +459,9 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
     v[u].y = 0;
     if (valid) v[u] = W[base + (int64_t)(t + Q::TPC * u) * g.h];
   }
-  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; }, taby, -1);
+  const int rb = Q::rd_base(t, b);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; },
+             [&](int u) { return &ex[Q::rd(rb, t, b, u)]; }, taby, -1);
   if (valid) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) W[base + (int64_t)(t + Q::TPC * u) * g.h] = v[u];
@@ -477,7 +489,9 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
     v[u].y = 0;
     if (valid) v[u] = Wr[base + (int64_t)(t + Q::TPC * u) * g.h];
   }
-  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; }, taby, +1);
+  const int rb = Q::rd_base(t, b);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; },
+             [&](int u) { return &ex[Q::rd(rb, t, b, u)]; }, taby, +1);
   if (!valid) return;
   const int64_t obase = (int64_t)ri * g.rs * g.h + kz0 + b;
 #pragma unroll
@@ -524,7 +538,9 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
       if (valid) gv[u] = G[base + (t + Q::TPC * u) * stride];
     }
   }
-  reg_fft<L>(v, t, exf, tabx, -1);
+  const int rb = Q::rd_base(t, b);
+  auto exr = [&](int u) { return &ex[Q::rd(rb, t, b, u)]; };
+  reg_fft<L>(v, t, exf, exr, tabx, -1);
   if constexpr (MODE == 0) {
     if (valid) {
 #pragma unroll
@@ -557,7 +573,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
       }
       __syncthreads();
     }
-    reg_fft<L>(v, t, exf, tabx, +1);
+    reg_fft<L>(v, t, exf, exr, tabx, +1);
     if (valid) {
       const int64_t obase = (int64_t)yy * g.h + kzi;
 #pragma unroll
@@ -719,6 +735,13 @@ struct PP {
   __device__ static __forceinline__ int row(int i) {
     return i ^ ((i >> 3) & (R - 1));
   }
+  static constexpr bool kFastRead = (TPC / 8) % R == 0;
+  __device__ static __forceinline__ int rd_base(int t, int p) {
+    return kFastRead ? row(t) * PB + p : 0;
+  }
+  __device__ static __forceinline__ int rd(int base, int t, int p, int u) {
+    return kFastRead ? base + u * TPC * PB : row(t + TPC * u) * PB + p;
+  }
 };
 
 template <int L>
@@ -740,7 +763,9 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
     const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
     v[u] = cpack(v0 ? W[r + c0] : zero, v1 ? W[r + c1] : zero);
   }
-  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; }, taby, -1);
+  const int rb = Q::rd_base(t, p);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
+             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, -1);
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
@@ -769,7 +794,9 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
     const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
     v[u] = cpack(v0 ? Wr[r + c0] : zero, v1 ? Wr[r + c1] : zero);
   }
-  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; }, taby, +1);
+  const int rb = Q::rd_base(t, p);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
+             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, +1);
   const int64_t obase = (int64_t)ri * g.rs * g.h;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
