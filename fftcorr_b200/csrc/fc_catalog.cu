@@ -261,7 +261,26 @@ void catalog_uniform(double *posw, int64_t first, int64_t n, const double lo[3],
   FC_LAUNCH_CHECK();
 }
 
-void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s) {
+size_t catalog_scratch_bytes(const fc_catalog_spec &c) {
+  const bool clustered =
+      c.kind == FC_CAT_CLUSTERED_BOX || c.kind == FC_CAT_SECTOR_CLUSTERED;
+  return clustered && c.ncentres > 0 ? (size_t)c.ncentres * 4 * sizeof(double)
+                                     : 0;
+}
+
+void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s,
+                      double *scratch, size_t scratch_bytes) {
+  // Cluster centres go to the caller's scratch when it is large enough, else
+  // to a stream-ordered allocation.
+  auto centres_buffer = [&](size_t bytes) {
+    double *p = nullptr;
+    if (scratch && scratch_bytes >= bytes) return scratch;
+    FC_CUDA(cudaMallocAsync(&p, bytes, s));
+    return p;
+  };
+  auto release = [&](double *p) {
+    if (p != scratch) FC_CUDA(cudaFreeAsync(p, s));
+  };
   const int64_t n = c.n;
   if (n <= 0) return;
   switch (c.kind) {
@@ -284,8 +303,7 @@ void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s) {
     case FC_CAT_CLUSTERED_BOX: {
       FC_REQUIRE(c.ncentres > 0, FC_ERR_INVALID, "ncentres must be positive");
       // Stream-ordered scratch: no device-wide synchronisation.
-      double *centres = nullptr;
-      FC_CUDA(cudaMallocAsync(&centres, (size_t)c.ncentres * 3 * sizeof(double), s));
+      double *centres = centres_buffer((size_t)c.ncentres * 3 * sizeof(double));
       k_centres<<<gen_blocks(c.ncentres), 256, 0, s>>>(centres, c.ncentres,
                                                        c.boxsize, c.seed);
       FC_LAUNCH_CHECK();
@@ -293,7 +311,7 @@ void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s) {
                                                 c.boxsize, c.sigma, c.wmin,
                                                 c.wmax, c.seed);
       FC_LAUNCH_CHECK();
-      FC_CUDA(cudaFreeAsync(centres, s));
+      release(centres);
       return;
     }
     case FC_CAT_SECTOR_UNIFORM:
@@ -304,8 +322,7 @@ void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s) {
       return;
     case FC_CAT_SECTOR_CLUSTERED: {
       FC_REQUIRE(c.ncentres > 0, FC_ERR_INVALID, "ncentres must be positive");
-      double *centres = nullptr;
-      FC_CUDA(cudaMallocAsync(&centres, (size_t)c.ncentres * 4 * sizeof(double), s));
+      double *centres = centres_buffer((size_t)c.ncentres * 4 * sizeof(double));
       k_sector<<<gen_blocks(c.ncentres), 256, 0, s>>>(
           centres, 0, c.ncentres, c.rmin, c.rmax, c.ra_half, c.dec_half, 1.0,
           1.0, 1.0, c.seed ^ 0x3c6ef372fe94f82bull);
@@ -314,7 +331,7 @@ void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s) {
           posw, n, centres, c.ncentres, c.sigma, c.rmin, c.rmax, c.ra_half,
           c.dec_half, c.wmin, c.wmax, c.wsign, c.seed);
       FC_LAUNCH_CHECK();
-      FC_CUDA(cudaFreeAsync(centres, s));
+      release(centres);
       return;
     }
   }

@@ -90,7 +90,11 @@ void catalog_uniform(double *posw, int64_t first, int64_t n, const double lo[3],
                      const double hi[3], double w0, double w1, uint64_t seed,
                      cudaStream_t s);
 // Writes the catalog a spec describes into posw (n rows of x, y, z, w).
-void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s);
+// scratch (optional): device memory for cluster centres, at least
+// catalog_scratch_bytes(c), so the call allocates nothing.
+void catalog_generate(const fc_catalog_spec &c, double *posw, cudaStream_t s,
+                      double *scratch = nullptr, size_t scratch_bytes = 0);
+size_t catalog_scratch_bytes(const fc_catalog_spec &c);
 // out[i] = pos[i] + disp[cell of pos[i]]; *flag = 1 if some position has no
 // cell.  Rows of pos and out are `stride` / `out_stride` doubles apart.
 void displace(const double *pos, int stride, int64_t n, const double *disp,

@@ -113,6 +113,14 @@ int64_t max_particles(const fc_job &j) {
   return std::max(j.data.n, j.kind == FC_SURVEY ? j.randoms.n : (int64_t)0);
 }
 
+// Device bytes of a worker's catalog staging for job j: the largest catalog
+// plus scratch for its cluster centres.
+size_t job_stage_bytes(const fc_job &j) {
+  const size_t cs = std::max(catalog_scratch_bytes(j.data),
+                             j.kind == FC_SURVEY ? catalog_scratch_bytes(j.randoms) : 0);
+  return ((size_t)max_particles(j) * 32 + 255) / 256 * 256 + cs;
+}
+
 void validate(const fc_job &j) {
   FC_REQUIRE(j.kind == FC_PERIODIC || j.kind == FC_SURVEY, FC_ERR_INVALID,
              "unknown job kind");
@@ -141,7 +149,7 @@ size_t job_footprint(const fc_job &j) {
   size_t b = ngrids * (grid_bytes(j) + assignor_bytes(j.shape, max_particles(j)));
   b += correlator_footprint(j.kind, j.shape, j.cell, j.rmax, j.kmax, j.maxell,
                             j.precision);
-  b += (size_t)max_particles(j) * 32;
+  b += job_stage_bytes(j);
   return b;
 }
 
@@ -239,7 +247,7 @@ struct Server {
       extra += correlator_footprint(s.kind, s.shape, s.cell, s.rmax, s.kmax,
                                     s.maxell, s.precision);
     // The worker's staging grows to the largest catalog it has seen.
-    const size_t need_stage = (size_t)need_n * 32;
+    const size_t need_stage = job_stage_bytes(s);
     const size_t grow_stage = need_stage > stage_bytes[slot] ? need_stage - stage_bytes[slot] : 0;
     extra += grow_stage;
     // Idle residents not reused here can be evicted.
@@ -421,14 +429,18 @@ struct Server {
                                 s.precision);
     Grid *ga = grids[0]->grid.get();
     const int64_t nmax = max_particles(s);
-    stage[slot]->resize(std::max<size_t>((size_t)nmax * 32, 32));
+    const size_t cs = std::max(catalog_scratch_bytes(s.data),
+                               s.kind == FC_SURVEY ? catalog_scratch_bytes(s.randoms) : 0);
+    const size_t nbuf = ((size_t)nmax * 32 + 255) / 256 * 256;
+    stage[slot]->resize(std::max<size_t>(nbuf + cs, 32));
     double *buf = stage[slot]->as<double>();
+    double *scr = reinterpret_cast<double *>(stage[slot]->as<char>() + nbuf);
     cudaStream_t st = ga->stream;
     lap(7);
     // Data grid.
     ga->clear();
     assignor_clear(grids[0]->ma);
-    catalog_generate(s.data, buf, st);
+    catalog_generate(s.data, buf, st, scr, cs);
     FC_CUDA(cudaStreamSynchronize(st));
     lap(0);
     assignor_add_device(grids[0]->ma, buf, s.data.n);
@@ -451,7 +463,7 @@ struct Server {
     gb->clear();
     assignor_clear(grids[1]->ma);
     stream_after(gb->stream, st);
-    catalog_generate(s.randoms, buf, gb->stream);
+    catalog_generate(s.randoms, buf, gb->stream, scr, cs);
     FC_CUDA(cudaStreamSynchronize(gb->stream));
     lap(2);
     assignor_add_device(grids[1]->ma, buf, s.randoms.n);
