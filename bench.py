@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--only-served", action="store_true")
     ap.add_argument("--served-jobs", type=int, default=24)
-    ap.add_argument("--served-slots", type=int, default=3)
+    ap.add_argument("--served-slots", type=int, default=2)
     ap.add_argument("--mix-jobs", type=int, default=48)
     ap.add_argument("--mix-rate", type=float, default=6.0)
     return ap.parse_args()
@@ -443,8 +443,11 @@ def run_served_saturated(a, w, precision, timer):
     """All requests queued at once: device-timed throughput of the server."""
     from fftcorr_b200.serve import Server
     srv = Server(served_budget(), slots=a.served_slots)
-    warm = survey_job_spec(w, 900, precision)
-    srv.wait(srv.submit(warm))
+    # One warm-up job per slot, so every slot's resident objects exist.
+    warm = [srv.submit(survey_job_spec(w, 900 + i, precision))
+            for i in range(a.served_slots)]
+    for t in warm:
+        srv.wait(t)
     specs = [survey_job_spec(w, 1000 + 10 * i, precision) for i in range(a.served_jobs)]
     timer.start()
     tickets = [srv.submit(s) for s in specs]
