@@ -297,9 +297,9 @@ def kernel_profile(job, dD, nD, dR, nR):
 # --no-fp64 --no-cpu-baseline`; the pass kernels see the same grid as the
 # full workload (only the catalogs are smaller).  Summaries under profiles/.
 TRAFFIC_PER_LAUNCH_512 = {
-    "zfwd": 1027.39e6,
-    "yfwd": 1024.73e6,
-    "xcorr": 1325.90e6,
+    "zfwd": 1035.25e6,
+    "yfwd": 1025.13e6,
+    "xcorr": 1326.52e6,
 }
 
 
