@@ -10,17 +10,19 @@
 //   K-key     grid coordinates, skip/wrap, tile-major cell key, counters
 //   K-sort    CUB radix sort of (key, particle index): stable, so the order
 //             of particles inside a cell is their input order
-//   K-tiles   first sorted position of every 8x8x8 tile (binary search)
-//   K-scatter one CTA per tile.  NGP/CIC/TSC: a thread per home cell sums
-//             its particles' stencil products in registers, and every cell
-//             of the tile's footprint (tile + stencil halo) adds the home
-//             cells' sums in a fixed order.  D12 (8^3 taps): particles are
-//             staged in shared memory with their 1-D weights and every
-//             footprint cell sums its contributions in a fixed order (home
-//             cell, then sorted particle order).  Either way each footprint
-//             total is added to the grid once.  Tiles are processed in colour
-//             passes chosen so that footprints within one pass never
-//             overlap, so there are no atomics and the result is
+//   K-units   first sorted position of every scatter unit (binary search)
+//             and, per colour, the list of non-empty units
+//   K-scatter NGP/CIC/TSC: persistent CTAs per colour pass draw 2x8x8-cell
+//             units; a thread per home cell sums its particles' stencil
+//             products in registers, and the footprint (unit + stencil
+//             halo) takes the home cells' sums in W^3 ordered rounds.  D12
+//             (8^3 taps): one CTA per 8^3 tile; particles are staged in
+//             shared memory with their 1-D weights and every footprint cell
+//             sums its contributions in a fixed order (home cell, then
+//             sorted particle order).  Either way each footprint total is
+//             added to the grid once.  Units are processed in colour passes
+//             chosen so that footprints within one pass never overlap, so
+//             there are no atomics on the grid and the result is
 //             bit-reproducible run to run.
 #include <cub/cub.cuh>
 
@@ -60,8 +62,24 @@ struct AssignGeom {
   int nt[3];  // tiles per axis
   double posmin[3];
   double cell;
+  double rcell;  // 1 / cell, correctly rounded
+  int fast_div;  // cell and rcell are in [2^-400, 2^400]
   int periodic;
 };
+
+// a / g.cell, correctly rounded.  For |a| in [2^-400, 2^400] and a cell in
+// the same range the quotient is formed from the correctly rounded
+// reciprocal with one fused residual correction (Markstein, IBM J. Res.
+// Dev. 34(1), 1990: q = a*r, e = fma(-q, cell, a), q + e*r rounds to
+// nearest), which is the IEEE quotient; elsewhere it is a plain division.
+__device__ __forceinline__ double div_cell(double a, const AssignGeom &g) {
+  const double m = fabs(a);
+  if (g.fast_div && m >= 0x1p-400 && m <= 0x1p400) {
+    const double q = a * g.rcell;
+    return fma(fma(-q, g.cell, a), g.rcell, q);
+  }
+  return a / g.cell;
+}
 
 // config_space_grid.h:31-46 on the device.
 __device__ __forceinline__ bool dev_grid_coords(const double *p,
@@ -69,7 +87,7 @@ __device__ __forceinline__ bool dev_grid_coords(const double *p,
                                                 double x[3]) {
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
-    double xi = (p[i] - g.posmin[i]) / g.cell;
+    double xi = div_cell(p[i] - g.posmin[i], g);
     const double xmax = (double)g.n[i];
     if (xi < 0 || xi >= xmax) {
       if (!g.periodic) return false;
@@ -224,14 +242,14 @@ __global__ void k_pack(const double *pos, const double *w, double wconst,
   }
 }
 
-// K-tiles: tile_start[t] = first sorted index whose key >= t*512, for
-// t in [0, ntiles]; invalid keys (== ntiles*512) sort last.
+// K-units: start[u] = first sorted index whose key >= u * unit_cells, for
+// u in [0, nunits]; invalid keys (== nunits * unit_cells) sort last.
 template <typename KeyT>
-__global__ void k_tile_starts(const KeyT *keys, int64_t n, int64_t ntiles,
-                              uint32_t *tile_start) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t <= ntiles;
+__global__ void k_unit_starts(const KeyT *keys, int64_t n, int64_t nunits,
+                              int unit_cells, uint32_t *start) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t <= nunits;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const KeyT target = (KeyT)t * kTileCells;
+    const KeyT target = (KeyT)t * (KeyT)unit_cells;
     int64_t lo = 0, hi = n;
     while (lo < hi) {
       const int64_t mid = (lo + hi) >> 1;
@@ -240,19 +258,29 @@ __global__ void k_tile_starts(const KeyT *keys, int64_t n, int64_t ntiles,
       else
         hi = mid;
     }
-    tile_start[t] = (uint32_t)lo;
+    start[t] = (uint32_t)lo;
   }
 }
 
-// (tile, first particle, end) of every tile in colour order, so a scatter
-// CTA finds its work with one load.
-__global__ void k_tile_ranges(const uint32_t *__restrict__ tiles, int64_t nt,
-                              const uint32_t *__restrict__ tile_start,
+// The non-empty units of every colour as (unit, first particle, end),
+// packed at the front of the colour's slice of `ranges`; cnt[c] counts
+// them.  `units` lists the units in colour order, colour c owning
+// [coff[c], coff[c + 1]).  The order inside a slice does not matter: units
+// of one colour have disjoint footprints.
+__global__ void k_unit_ranges(const uint32_t *__restrict__ units, int64_t nu,
+                              const uint32_t *__restrict__ start,
+                              const int64_t *__restrict__ coff, int ncolors,
+                              unsigned *__restrict__ cnt,
                               uint4 *__restrict__ ranges) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nt;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nu;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t t = tiles[i];
-    ranges[i] = make_uint4(t, tile_start[t], tile_start[t + 1], 0u);
+    const uint32_t u = units[i];
+    const uint32_t ts = start[u], te = start[u + 1];
+    if (ts >= te) continue;
+    int c = 0;
+    while (c + 1 < ncolors && i >= coff[c + 1]) ++c;
+    const unsigned slot = atomicAdd(&cnt[c], 1u);
+    ranges[coff[c] + slot] = make_uint4(u, ts, te, 0u);
   }
 }
 
@@ -365,31 +393,52 @@ __global__ void __launch_bounds__(kScatterThreads)
   }
 }
 
-// K-scatter for stencils of width <= 3 (NGP, CIC, TSC): one thread per
-// home cell of the 8x8x8 tile.  The tile's particles (contiguous in sorted
-// order) are staged in chunks: all threads gather positions and weights in
-// parallel into shared memory (fractional cell offsets and weight), then
-// each thread walks its own cell's particles of the chunk in sorted order
-// and accumulates the W^3 products wx[a]*wy[b]*wz[c] in registers
-// (S_h[a][b][c]).  The sums go to shared memory, and every footprint cell
-// then adds the S_h[o] of the home cells h = f - o in a fixed order.  Each
-// cell's particles are summed in sorted order whatever the chunking, so the
-// grid is the same bits on every run.
-template <int S>
-struct ScatterS {
+// K-scatter for stencils of width <= 3 (NGP, CIC, TSC).  The work unit is
+// a sub-tile of TX x 8 x 8 home cells (TX = 2, 4 or 8: a contiguous range
+// of tile-major keys), one thread per home cell, and a colour pass is run
+// by persistent CTAs that draw the non-empty units of the colour from a
+// counter.  A unit's particles (contiguous in sorted order) are staged in
+// chunks: all threads gather positions and weights in parallel into shared
+// memory (fractional cell offsets and weight), then each thread walks its
+// own cell's particles of the chunk in sorted order and accumulates the W^3
+// products wx[a]*wy[b]*wz[c] in registers (S_h[a][b][c]).  The footprint
+// sums are then formed in W^3 rounds: in round o every home cell h adds
+// S_h[o] to footprint cell h + o, with a barrier between rounds, so each
+// footprint cell adds its terms in the order o.  Each cell's particles are
+// summed in sorted order whatever the chunking, so the grid is the same
+// bits on every run.
+// Scatter unit width along x for the narrow stencils: 2 x 8 x 8 home cells
+// per CTA of 128 threads, five CTAs per SM.
+constexpr int kUnitX = 2;
+
+template <int S, int TX>
+struct ScatterP {
   static constexpr int W = Stencil<S>::W;
   static constexpr int W3 = W * W * W;
-  static constexpr int F = kTile + W - 1;
-  static constexpr int F3 = F * F * F;
-  // Staged particles per chunk: at least 1024, more when the S_h buffer the
-  // chunk shares memory with is larger (TSC).
-  static constexpr int C0 = (W3 * kTileCells * 8) / 36 / 32 * 32;
-  static constexpr int C = C0 > 1024 ? C0 : 1024;
-  static constexpr size_t region =
-      (size_t)W3 * kTileCells * 8 > (size_t)C * 36 ? (size_t)W3 * kTileCells * 8
-                                                   : (size_t)C * 36;
-  static constexpr size_t smem = region + (size_t)F3 * 8;
+  static constexpr int THREADS = TX * 64;
+  static constexpr int MIN_BLOCKS = TX == 2 ? 5 : kTile / TX;
+  static constexpr int FX = TX + W - 1;     // footprint extent along x
+  static constexpr int FY = kTile + W - 1;  // ... along y and z
+  static constexpr int F3 = FX * FY * FY;
+  static constexpr int C = TX * 256;  // particles staged per chunk
+  // pd[C][4] | acc[F3] | gfoot[F3] doubles, pc[C] | cstart[THREADS + 1] ints
+  static constexpr size_t smem =
+      (size_t)C * 36 + (size_t)F3 * 16 + (size_t)(THREADS + 1) * 4;
 };
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
 
 __device__ __forceinline__ int lower_bound_smem(const int *a, int n, int v) {
   int lo = 0, hi = n;
@@ -400,158 +449,203 @@ __device__ __forceinline__ int lower_bound_smem(const int *a, int n, int v) {
   return lo;
 }
 
-template <int S, typename KeyT>
-__global__ void __launch_bounds__(kTileCells)
-    k_scatter_s(const double *__restrict__ posw, const KeyT *__restrict__ keys,
-                const uint32_t *__restrict__ vals,
-                const uint4 *__restrict__ ranges, AssignGeom g,
-                double *__restrict__ grid) {
-  using Q = ScatterS<S>;
-  constexpr int W = Q::W;
-  constexpr int OMIN = Stencil<S>::OMIN;
-  constexpr int W3 = Q::W3;
-  constexpr int F = Q::F;
-  constexpr int F3 = Q::F3;
-  constexpr int C = Q::C;
-  extern __shared__ double smem[];
-  double *sh = smem;                                   // [W3][512], last
-  double *pd = smem;                                   // [C][4], per chunk
-  int *pc = reinterpret_cast<int *>(smem + 4 * C);     // [C], per chunk
-  double *acc = smem + Q::region / 8;                  // [F3]
-
-  const uint4 rg = ranges[blockIdx.x];
-  const uint32_t tile = rg.x;
-  const uint32_t ts = rg.y;
-  const uint32_t te = rg.z;
-  if (ts >= te) return;
-  const int tz = tile % g.nt[2];
-  const int ty = (tile / g.nt[2]) % g.nt[1];
-  const int tx = tile / (g.nt[2] * g.nt[1]);
-  const int o0 = tx * kTile, o1 = ty * kTile, o2 = tz * kTile;
-  const int h = threadIdx.x;
-  const KeyT kbase = (KeyT)tile * kTileCells;
-  // When no footprint wraps onto itself, each footprint cell has one
-  // global cell: load its current value now, so the latency of the final
-  // read-modify-write overlaps the particle gather.  (No other CTA of this
-  // colour pass touches these cells.)
-  constexpr int kFPer = (F3 + kTileCells - 1) / kTileCells;
-  const bool direct = g.n[0] >= F && g.n[1] >= F && g.n[2] >= F;
-  size_t gidx[kFPer];
-  double gval[kFPer];
-#pragma unroll
-  for (int r = 0; r < kFPer; ++r) {
-    const int f = threadIdx.x + r * kTileCells;
-    gidx[r] = 0;
-    gval[r] = 0.0;
-    if (direct && f < F3) {
-      int gx = (o0 + f / (F * F) + OMIN) % g.n[0];
-      int gy = (o1 + (f / F) % F + OMIN) % g.n[1];
-      int gz = (o2 + f % F + OMIN) % g.n[2];
-      if (gx < 0) gx += g.n[0];
-      if (gy < 0) gy += g.n[1];
-      if (gz < 0) gz += g.n[2];
-      gidx[r] = ((size_t)gx * g.n[1] + gy) * g.n[2] + gz;
-      gval[r] = grid[gidx[r]];
-    }
-  }
-
-  double sacc[W3];
-#pragma unroll
-  for (int o = 0; o < W3; ++o) sacc[o] = 0.0;
-  for (uint32_t c0 = ts; c0 < te; c0 += C) {
-    const int m = (int)min((uint32_t)C, te - c0);
-    if (c0 != ts) __syncthreads();  // the previous chunk has been consumed
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-      const uint32_t q = c0 + i;
-      const double *p = posw + 4 * (size_t)vals[q];
-      double x[3];
-      dev_grid_coords(p, g, x);
-      pd[4 * i + 0] = x[0] - home_cell(x[0], g.n[0]);
-      pd[4 * i + 1] = x[1] - home_cell(x[1], g.n[1]);
-      pd[4 * i + 2] = x[2] - home_cell(x[2], g.n[2]);
-      pd[4 * i + 3] = p[3];
-      pc[i] = (int)(keys[q] - kbase);
-    }
-    __syncthreads();
-    const int lo = lower_bound_smem(pc, m, h);
-    const int hi = lower_bound_smem(pc, m, h + 1);
-    for (int i = lo; i < hi; ++i) {
-      double wx[W], wy[W], wz[W];
-      Stencil<S>::weights(pd[4 * i + 0], pd[4 * i + 1], pd[4 * i + 2],
-                          pd[4 * i + 3], wx, wy, wz);
-#pragma unroll
-      for (int a = 0; a < W; ++a)
-#pragma unroll
-        for (int b = 0; b < W; ++b) {
-          const double wxy = wx[a] * wy[b];
-#pragma unroll
-          for (int c = 0; c < W; ++c) sacc[(a * W + b) * W + c] += wxy * wz[c];
-        }
-    }
-  }
-  __syncthreads();  // the chunk buffer becomes S_h
-#pragma unroll
-  for (int o = 0; o < W3; ++o) sh[o * kTileCells + h] = sacc[o];
-  __syncthreads();
-  for (int f = threadIdx.x; f < F3; f += blockDim.x) {
-    const int fx = f / (F * F);
-    const int fy = (f / F) % F;
-    const int fz = f % F;
-    double a = 0.0;
-#pragma unroll
-    for (int ox = 0; ox < W; ++ox) {
-      const int hx = fx - ox;
-      if (hx < 0 || hx >= kTile) continue;
-#pragma unroll
-      for (int oy = 0; oy < W; ++oy) {
-        const int hy = fy - oy;
-        if (hy < 0 || hy >= kTile) continue;
-#pragma unroll
-        for (int oz = 0; oz < W; ++oz) {
-          const int hz = fz - oz;
-          if (hz < 0 || hz >= kTile) continue;
-          a += sh[((ox * W + oy) * W + oz) * kTileCells + (hx * 64 + hy * 8 + hz)];
-        }
-      }
-    }
-    acc[f] = a;
-  }
-  __syncthreads();
-  if (direct) {
-#pragma unroll
-    for (int r = 0; r < kFPer; ++r) {
-      const int f = threadIdx.x + r * kTileCells;
-      if (f >= F3) continue;
-      const double v = 0.0 + acc[f];
-      if (v != 0.0) grid[gidx[r]] = gval[r] + v;
-    }
-    return;
-  }
-  // Each global cell is written by one footprint cell (its smallest alias
-  // when the footprint wraps onto itself on grids narrower than F).
-  for (int f = threadIdx.x; f < F3; f += blockDim.x) {
-    const int fx = f / (F * F);
-    const int fy = (f / F) % F;
-    const int fz = f % F;
-    if (fx >= g.n[0] || fy >= g.n[1] || fz >= g.n[2]) continue;
-    double v = 0.0;
-    for (int ax = fx; ax < F; ax += g.n[0])
-      for (int ay = fy; ay < F; ay += g.n[1])
-        for (int az = fz; az < F; az += g.n[2]) v += acc[(ax * F + ay) * F + az];
-    if (v == 0.0) continue;
-    int gx = (o0 + fx + OMIN) % g.n[0];
-    int gy = (o1 + fy + OMIN) % g.n[1];
-    int gz = (o2 + fz + OMIN) % g.n[2];
-    if (gx < 0) gx += g.n[0];
-    if (gy < 0) gy += g.n[1];
-    if (gz < 0) gz += g.n[2];
-    grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz] += v;
-  }
+// Global cell of footprint cell (fx, fy, fz) of a unit at (o0, o1, o2) on a
+// grid at least a footprint wide (one wrap at most per axis).
+template <int OMIN>
+__device__ __forceinline__ size_t foot_cell(int fx, int fy, int fz, int o0,
+                                            int o1, int o2,
+                                            const AssignGeom &g) {
+  int gx = o0 + fx + OMIN, gy = o1 + fy + OMIN, gz = o2 + fz + OMIN;
+  gx += gx < 0 ? g.n[0] : (gx >= g.n[0] ? -g.n[0] : 0);
+  gy += gy < 0 ? g.n[1] : (gy >= g.n[1] ? -g.n[1] : 0);
+  gz += gz < 0 ? g.n[2] : (gz >= g.n[2] ? -g.n[2] : 0);
+  return ((size_t)gx * g.n[1] + gy) * g.n[2] + gz;
 }
 
-template <int S>
-size_t scatter_s_smem() {
-  return ScatterS<S>::smem;
+// ranges: this colour's non-empty units (unit, first, end), `count` of
+// them; `next` is this colour's work counter (zero before the pass).
+template <int S, typename KeyT, int TX>
+__global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
+    k_scatter_p(const double *__restrict__ posw, const KeyT *__restrict__ keys,
+                const uint32_t *__restrict__ vals,
+                const uint4 *__restrict__ ranges,
+                const unsigned *__restrict__ count, unsigned *next,
+                AssignGeom g, double *__restrict__ grid) {
+  using Q = ScatterP<S, TX>;
+  constexpr int W = Q::W;
+  constexpr int W3 = Q::W3;
+  constexpr int T = Q::THREADS;
+  constexpr int FX = Q::FX;
+  constexpr int FY = Q::FY;
+  constexpr int F3 = Q::F3;
+  constexpr int C = Q::C;
+  constexpr int NS = kTile / TX;
+  constexpr int OMIN = Stencil<S>::OMIN;
+  constexpr int kSlots = C / T;
+  static_assert(C % T == 0, "whole staging slots per thread");
+  extern __shared__ __align__(16) double smem[];
+  double *pd = smem;                                     // [C][4]
+  double *acc = pd + 4 * C;                              // [F3]
+  double *gfoot = acc + F3;                              // [F3]
+  int *pc = reinterpret_cast<int *>(gfoot + F3);         // [C]
+  int *cstart = pc + C;                                  // [T + 1]
+  __shared__ uint4 s_rg;
+  __shared__ unsigned s_next;
+
+  const unsigned n = *count;
+  if (threadIdx.x == 0) {
+    const unsigned i0 = atomicAdd(next, 1u);
+    s_next = atomicAdd(next, 1u);
+    s_rg = i0 < n ? ranges[i0] : make_uint4(0u, 0u, 0u, 0u);
+  }
+  __syncthreads();
+  uint4 rg = s_rg;
+  unsigned inext = s_next;
+  const int h = threadIdx.x;
+  const int hx = h >> 6, hy = (h >> 3) & 7, hz = h & 7;
+  const bool direct = g.n[0] >= FX && g.n[1] >= FY && g.n[2] >= FY;
+  const bool a16 = (reinterpret_cast<uintptr_t>(posw) & 15) == 0;
+  while (rg.y < rg.z) {
+    // Thread 0 fetches the next unit's range and draws the index after it;
+    // neither is needed before the end of this unit.
+    uint4 rgn = make_uint4(0u, 0u, 0u, 0u);
+    unsigned inn = 0;
+    if (threadIdx.x == 0) {
+      inn = atomicAdd(next, 1u);
+      if (inext < n) rgn = ranges[inext];
+    }
+    const uint32_t unit = rg.x, ts = rg.y, te = rg.z;
+    const uint32_t tile = unit / NS;
+    const int tz = tile % g.nt[2];
+    const int ty = (tile / g.nt[2]) % g.nt[1];
+    const int tx = tile / (g.nt[2] * g.nt[1]);
+    const int o0 = tx * kTile + (int)(unit % NS) * TX;
+    const int o1 = ty * kTile, o2 = tz * kTile;
+    const KeyT kbase = (KeyT)unit * (KeyT)T;
+    // When no footprint wraps onto itself, each footprint cell has one
+    // global cell: copy its current value now, so the latency of the final
+    // read-modify-write overlaps the particle gather.  (No other CTA of this
+    // colour pass touches these cells.)  The first chunk's wait covers it.
+    for (int f = h; f < F3; f += T) {
+      acc[f] = 0.0;
+      if (direct)
+        cp_async8(gfoot + f, grid + foot_cell<OMIN>(f / (FY * FY), (f / FY) % FY,
+                                                    f % FY, o0, o1, o2, g));
+    }
+
+    double sacc[W3];
+#pragma unroll
+    for (int o = 0; o < W3; ++o) sacc[o] = 0.0;
+    for (uint32_t c0 = ts; c0 < te; c0 += C) {
+      const int m = (int)min((uint32_t)C, te - c0);
+      if (c0 != ts) __syncthreads();  // the previous chunk has been consumed
+      // Each thread stages up to kSlots particles: all index and key loads
+      // first, then the position gathers as asynchronous copies, so the
+      // gathers of one thread overlap.  Each thread converts its own copies.
+      uint32_t idx[kSlots];
+      KeyT kk[kSlots];
+#pragma unroll
+      for (int j = 0; j < kSlots; ++j) {
+        const int i = h + j * T;
+        idx[j] = 0u;
+        kk[j] = kbase;
+        if (i < m) {
+          idx[j] = vals[c0 + i];
+          kk[j] = keys[c0 + i];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kSlots; ++j) {
+        const int i = h + j * T;
+        if (i >= m) continue;
+        const double *p = posw + 4 * (size_t)idx[j];
+        double *d = pd + 4 * i;
+        if (a16) {
+          cp_async16(d, p);
+          cp_async16(d + 2, p + 2);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) cp_async8(d + k, p + k);
+        }
+        pc[i] = (int)(kk[j] - kbase);
+      }
+      cp_async_wait_all();
+#pragma unroll
+      for (int j = 0; j < kSlots; ++j) {
+        const int i = h + j * T;
+        if (i >= m) continue;
+        double *d = pd + 4 * i;
+        double x[3];
+        dev_grid_coords(d, g, x);
+        d[0] = x[0] - home_cell(x[0], g.n[0]);
+        d[1] = x[1] - home_cell(x[1], g.n[1]);
+        d[2] = x[2] - home_cell(x[2], g.n[2]);
+      }
+      __syncthreads();  // also orders the zeroing of acc before round 0
+      cstart[h] = lower_bound_smem(pc, m, h);
+      if (h == 0) cstart[T] = m;
+      __syncthreads();
+      const int lo = cstart[h], hi = cstart[h + 1];
+      for (int i = lo; i < hi; ++i) {
+        double wx[W], wy[W], wz[W];
+        Stencil<S>::weights(pd[4 * i + 0], pd[4 * i + 1], pd[4 * i + 2],
+                            pd[4 * i + 3], wx, wy, wz);
+#pragma unroll
+        for (int a = 0; a < W; ++a)
+#pragma unroll
+          for (int b = 0; b < W; ++b) {
+            const double wxy = wx[a] * wy[b];
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+              sacc[(a * W + b) * W + c] = fma(wxy, wz[c], sacc[(a * W + b) * W + c]);
+          }
+      }
+    }
+    // Within a round the targets h + o are distinct.
+#pragma unroll
+    for (int o = 0; o < W3; ++o) {
+      const int ox = o / (W * W), oy = (o / W) % W, oz = o % W;
+      acc[((hx + ox) * FY + (hy + oy)) * FY + (hz + oz)] += sacc[o];
+      __syncthreads();
+    }
+    if (direct) {
+      for (int f = h; f < F3; f += T) {
+        const double v = 0.0 + acc[f];
+        if (v != 0.0)
+          grid[foot_cell<OMIN>(f / (FY * FY), (f / FY) % FY, f % FY, o0, o1, o2,
+                               g)] = gfoot[f] + v;
+      }
+    } else {
+      // Each global cell is written by one footprint cell (its smallest
+      // alias when the footprint wraps onto itself on narrow grids).
+      for (int f = h; f < F3; f += T) {
+        const int fx = f / (FY * FY);
+        const int fy = (f / FY) % FY;
+        const int fz = f % FY;
+        if (fx >= g.n[0] || fy >= g.n[1] || fz >= g.n[2]) continue;
+        double v = 0.0;
+        for (int ax = fx; ax < FX; ax += g.n[0])
+          for (int ay = fy; ay < FY; ay += g.n[1])
+            for (int az = fz; az < FY; az += g.n[2])
+              v += acc[(ax * FY + ay) * FY + az];
+        if (v == 0.0) continue;
+        int gx = (o0 + fx + OMIN) % g.n[0];
+        int gy = (o1 + fy + OMIN) % g.n[1];
+        int gz = (o2 + fz + OMIN) % g.n[2];
+        if (gx < 0) gx += g.n[0];
+        if (gy < 0) gy += g.n[1];
+        if (gz < 0) gz += g.n[2];
+        grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz] += v;
+      }
+    }
+    if (threadIdx.x == 0) {
+      s_rg = rgn;
+      s_next = inn;
+    }
+    __syncthreads();  // acc and the staging buffers are free again
+    rg = s_rg;
+    inext = s_next;
+  }
 }
 
 template <int S>
@@ -562,33 +656,29 @@ size_t scatter_smem() {
          sizeof(int) * (kChunk + kTileCells + 1);
 }
 
-// Greedy colouring of the tiles along one axis so that tiles sharing a
-// colour have disjoint (periodically wrapped) footprints.
-std::vector<int> color_axis(int n, int ntiles, int W, int omin) {
-  std::vector<std::vector<char>> cover(ntiles, std::vector<char>(n, 0));
-  for (int t = 0; t < ntiles; ++t) {
-    const int lo = t * kTile;
-    const int hi = std::min(n, lo + kTile) - 1;
+// Greedy colouring along one axis of units `unit` cells wide, so that
+// units sharing a colour have disjoint (periodically wrapped) footprints.
+// Units past the end of the axis hold no cells and take colour 0.
+std::vector<int> color_axis(int n, int nunits, int unit, int W, int omin) {
+  std::vector<std::vector<char>> used;  // per colour: cells covered so far
+  std::vector<int> color(nunits, 0);
+  std::vector<char> cover(n);
+  for (int t = 0; t < nunits; ++t) {
+    const int lo = t * unit;
+    if (lo >= n) continue;
+    const int hi = std::min(n, lo + unit) - 1;
+    std::fill(cover.begin(), cover.end(), 0);
     for (int c = lo + omin; c <= hi + omin + W - 1; ++c)
-      cover[t][((c % n) + n) % n] = 1;
-  }
-  std::vector<int> color(ntiles, -1);
-  for (int t = 0; t < ntiles; ++t) {
-    for (int c = 0;; ++c) {
+      cover[((c % n) + n) % n] = 1;
+    int c = 0;
+    for (;; ++c) {
+      if (c == (int)used.size()) used.emplace_back(n, 0);
       bool ok = true;
-      for (int u = 0; u < t && ok; ++u) {
-        if (color[u] != c) continue;
-        for (int k = 0; k < n; ++k)
-          if (cover[t][k] && cover[u][k]) {
-            ok = false;
-            break;
-          }
-      }
-      if (ok) {
-        color[t] = c;
-        break;
-      }
+      for (int k = 0; k < n && ok; ++k) ok = !(cover[k] && used[c][k]);
+      if (ok) break;
     }
+    for (int k = 0; k < n; ++k) used[c][k] |= cover[k];
+    color[t] = c;
   }
   return color;
 }
@@ -610,6 +700,25 @@ int stencil_width(int scheme, int *omin) {
   }
 }
 
+// Scatter kernel for scheme 0, 1 or 3 and a key type.
+template <typename KeyT>
+void scatter_p_kernel(int scheme, const void **fn, size_t *smem) {
+  switch (scheme) {
+    case 0:
+      *fn = (const void *)k_scatter_p<0, KeyT, kUnitX>;
+      *smem = ScatterP<0, kUnitX>::smem;
+      break;
+    case 1:
+      *fn = (const void *)k_scatter_p<1, KeyT, kUnitX>;
+      *smem = ScatterP<1, kUnitX>::smem;
+      break;
+    default:
+      *fn = (const void *)k_scatter_p<3, KeyT, kUnitX>;
+      *smem = ScatterP<3, kUnitX>::smem;
+      break;
+  }
+}
+
 }  // namespace
 
 // MassAssignor state (mass_assignor.h:30-234) with a device-side buffer.
@@ -620,6 +729,8 @@ struct Assignor {
   int64_t buffer_size;
   AssignGeom geom;
   int64_t ntiles;
+  int unit_x;      // scatter unit: unit_x x 8 x 8 cells
+  int64_t nunits;  // ntiles * (8 / unit_x)
   bool wide_keys;  // 64-bit keys when the key space exceeds 32 bits
   int end_bit;
 
@@ -627,10 +738,16 @@ struct Assignor {
   int64_t count = 0;
   int64_t capacity = 0;
   DeviceBuffer posw, keys, keys_alt, vals, vals_alt, cub_temp;
-  DeviceBuffer tile_start;
-  DeviceBuffer color_tiles;
-  DeviceBuffer tile_ranges;            // uint4 per tile, colour order
-  std::vector<int64_t> color_offsets;  // per colour, into color_tiles
+  DeviceBuffer unit_start;             // first sorted particle per unit
+  DeviceBuffer color_units;            // units in colour order
+  DeviceBuffer unit_ranges;            // uint4 per unit, colour slices
+  DeviceBuffer color_off_dev;          // color_offsets on the device
+  DeviceBuffer pass_counters;          // per colour: non-empty units, work
+  std::vector<int64_t> color_offsets;  // per colour, into color_units
+  const void *scatter_fn = nullptr;    // k_scatter_p for this scheme / keys
+  size_t scatter_smem_bytes = 0;
+  int scatter_threads = 0;
+  unsigned scatter_ctas = 0;           // persistent CTAs per colour pass
   DeviceBuffer partials;               // K-key block partials
   DeviceBuffer totals;                 // [totw, totwsq]
   DeviceBuffer counts;                 // [num_added]
@@ -660,28 +777,38 @@ struct Assignor {
       geom.posmin[i] = g->posmin[i];
     }
     geom.cell = g->cell_size;
+    geom.rcell = 1.0 / geom.cell;
+    geom.fast_div = geom.cell >= 0x1p-400 && geom.cell <= 0x1p400;
     geom.periodic = periodic ? 1 : 0;
     ntiles = (int64_t)geom.nt[0] * geom.nt[1] * geom.nt[2];
+    unit_x = scheme == 2 ? kTile : kUnitX;
+    nunits = ntiles * (kTile / unit_x);
     const uint64_t max_key = (uint64_t)ntiles * kTileCells;  // invalid key
     wide_keys = max_key >= 0xffffffffull;
     end_bit = 1;
     while (end_bit < 64 && (max_key >> end_bit) != 0) ++end_bit;
-    tile_start.resize((ntiles + 1) * sizeof(uint32_t));
-    tile_ranges.resize(std::max<int64_t>(ntiles, 1) * sizeof(uint4));
+    unit_start.resize((nunits + 1) * sizeof(uint32_t));
+    if (scheme != 2) unit_ranges.resize(std::max<int64_t>(nunits, 1) * sizeof(uint4));
     partials.resize(2 * kSumBlocks * sizeof(double));
     totals.resize(2 * sizeof(double));
     counts.resize(sizeof(unsigned long long));
     build_colors();
     FC_CUDA(cudaMemsetAsync(totals.get(), 0, totals.bytes(), grid->stream));
     FC_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), grid->stream));
-    for (auto fn : {(const void *)k_scatter_s<0, uint32_t>,
-                    (const void *)k_scatter_s<0, uint64_t>,
-                    (const void *)k_scatter_s<1, uint32_t>,
-                    (const void *)k_scatter_s<1, uint64_t>,
-                    (const void *)k_scatter_s<3, uint32_t>,
-                    (const void *)k_scatter_s<3, uint64_t>})
-      FC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)scatter_s_smem<1>()));
+    if (scheme != 2) {
+      if (wide_keys)
+        scatter_p_kernel<uint64_t>(scheme, &scatter_fn, &scatter_smem_bytes);
+      else
+        scatter_p_kernel<uint32_t>(scheme, &scatter_fn, &scatter_smem_bytes);
+      scatter_threads = unit_x * 64;
+      FC_CUDA(cudaFuncSetAttribute(scatter_fn,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)scatter_smem_bytes));
+      int per_sm = 0;
+      FC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, scatter_fn, scatter_threads, scatter_smem_bytes));
+      scatter_ctas = (unsigned)std::max(1, per_sm) * (unsigned)sm_count();
+    }
     if (scheme == 2) {
       FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -703,31 +830,39 @@ struct Assignor {
   void build_colors() {
     int omin = 0;
     const int W = stencil_width(scheme, &omin);
+    const int ns = kTile / unit_x;
+    const int nux[3] = {geom.nt[0] * ns, geom.nt[1], geom.nt[2]};
+    const int unit[3] = {unit_x, kTile, kTile};
     std::vector<int> col[3];
     int ncol[3];
     for (int a = 0; a < 3; ++a) {
-      col[a] = color_axis(geom.n[a], geom.nt[a], W, omin);
+      col[a] = color_axis(geom.n[a], nux[a], unit[a], W, omin);
       ncol[a] = 1 + *std::max_element(col[a].begin(), col[a].end());
     }
     const int ncolors = ncol[0] * ncol[1] * ncol[2];
     std::vector<std::vector<uint32_t>> lists(ncolors);
-    for (int tx = 0; tx < geom.nt[0]; ++tx)
+    for (int ux = 0; ux < nux[0]; ++ux)
       for (int ty = 0; ty < geom.nt[1]; ++ty)
         for (int tz = 0; tz < geom.nt[2]; ++tz) {
-          const int c = (col[0][tx] * ncol[1] + col[1][ty]) * ncol[2] + col[2][tz];
-          lists[c].push_back(
-              (uint32_t)(((int64_t)tx * geom.nt[1] + ty) * geom.nt[2] + tz));
+          const int c = (col[0][ux] * ncol[1] + col[1][ty]) * ncol[2] + col[2][tz];
+          const int64_t tile = ((int64_t)(ux / ns) * geom.nt[1] + ty) * geom.nt[2] + tz;
+          lists[c].push_back((uint32_t)(tile * ns + ux % ns));
         }
     std::vector<uint32_t> flat;
-    flat.reserve(ntiles);
+    flat.reserve(nunits);
     color_offsets.assign(1, 0);
     for (auto &l : lists) {
       flat.insert(flat.end(), l.begin(), l.end());
       color_offsets.push_back((int64_t)flat.size());
     }
-    color_tiles.resize(flat.size() * sizeof(uint32_t));
-    FC_CUDA(cudaMemcpy(color_tiles.get(), flat.data(),
+    color_units.resize(flat.size() * sizeof(uint32_t));
+    FC_CUDA(cudaMemcpy(color_units.get(), flat.data(),
                        flat.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    color_off_dev.resize(color_offsets.size() * sizeof(int64_t));
+    FC_CUDA(cudaMemcpy(color_off_dev.get(), color_offsets.data(),
+                       color_offsets.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice));
+    pass_counters.resize(2 * ncolors * sizeof(unsigned));
   }
 
   size_t key_bytes() const { return wide_keys ? 8 : 4; }
@@ -902,45 +1037,44 @@ struct Assignor {
     if (!graph_mode) sort_timer.stop(stream());
     const KeyT *sk = dk.Current();
     const uint32_t *sv = dv.Current();
-    // K-tiles + K-scatter.
+    // K-units + K-scatter.
     if (!graph_mode) window_timer.start(stream());
-    k_tile_starts<KeyT><<<grid_for(ntiles + 1, 256), 256, 0, stream()>>>(
-        sk, n, ntiles, tile_start.as<uint32_t>());
+    const int unit_cells = unit_x * kTile * kTile;
+    k_unit_starts<KeyT><<<grid_for(nunits + 1, 256), 256, 0, stream()>>>(
+        sk, n, nunits, unit_cells, unit_start.as<uint32_t>());
     FC_LAUNCH_CHECK();
-    const uint32_t *tiles = color_tiles.as<uint32_t>();
+    const uint32_t *units = color_units.as<uint32_t>();
+    const int ncolors = (int)color_offsets.size() - 1;
+    unsigned *counters = pass_counters.as<unsigned>();
     if (scheme != 2) {
-      k_tile_ranges<<<grid_for(ntiles, 256), 256, 0, stream()>>>(
-          tiles, ntiles, tile_start.as<uint32_t>(), tile_ranges.as<uint4>());
+      FC_CUDA(cudaMemsetAsync(counters, 0, pass_counters.bytes(), stream()));
+      k_unit_ranges<<<grid_for(nunits, 256), 256, 0, stream()>>>(
+          units, nunits, unit_start.as<uint32_t>(), color_off_dev.as<int64_t>(),
+          ncolors, counters, unit_ranges.as<uint4>());
       FC_LAUNCH_CHECK();
     }
-    for (size_t c = 0; c + 1 < color_offsets.size(); ++c) {
-      const int64_t nt = color_offsets[c + 1] - color_offsets[c];
-      if (nt == 0) continue;
-      const uint32_t *ct = tiles + color_offsets[c];
-      const uint4 *cr = tile_ranges.as<uint4>() + color_offsets[c];
-      switch (scheme) {
-        case 0:
-          k_scatter_s<0, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<0>(),
-                                 stream()>>>(src_posw, sk, sv, cr, geom,
-                                             grid->ptr());
-          break;
-        case 1:
-          k_scatter_s<1, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<1>(),
-                                 stream()>>>(src_posw, sk, sv, cr, geom,
-                                             grid->ptr());
-          break;
-        case 2:
-          k_scatter<2, KeyT><<<(unsigned)nt, kScatterThreads, scatter_smem<2>(),
-                               stream()>>>(src_posw, sk, sv,
-                                           tile_start.as<uint32_t>(), ct, geom,
-                                           grid->ptr());
-          break;
-        default:
-          k_scatter_s<3, KeyT><<<(unsigned)nt, kTileCells, scatter_s_smem<3>(),
-                                 stream()>>>(src_posw, sk, sv, cr, geom,
-                                             grid->ptr());
-          break;
+    double *gp = grid->ptr();
+    AssignGeom ga = geom;
+    for (int c = 0; c < ncolors; ++c) {
+      const int64_t nu = color_offsets[c + 1] - color_offsets[c];
+      if (nu == 0) continue;
+      if (scheme == 2) {
+        k_scatter<2, KeyT><<<(unsigned)nu, kScatterThreads, scatter_smem<2>(),
+                             stream()>>>(src_posw, sk, sv,
+                                         unit_start.as<uint32_t>(),
+                                         units + color_offsets[c], geom, gp);
+        FC_LAUNCH_CHECK();
+        continue;
       }
+      const uint4 *cr = unit_ranges.as<uint4>() + color_offsets[c];
+      const unsigned *cnt = counters + c;
+      unsigned *nxt = counters + ncolors + c;
+      const double *pw = src_posw;
+      void *args[] = {(void *)&pw, (void *)&sk, (void *)&sv, (void *)&cr,
+                      (void *)&cnt, (void *)&nxt, (void *)&ga, (void *)&gp};
+      const unsigned ctas = (unsigned)std::min<int64_t>(nu, scatter_ctas);
+      FC_CUDA(cudaLaunchKernel(scatter_fn, dim3(ctas), dim3(scatter_threads),
+                               args, scatter_smem_bytes, stream()));
       FC_LAUNCH_CHECK();
     }
     if (!graph_mode) window_timer.stop(stream());
@@ -1096,7 +1230,8 @@ size_t assignor_bytes(const int shape[3], int64_t n) {
   for (int i = 0; i < 3; ++i) nt *= (shape[i] + kTile - 1) / kTile;
   const bool wide = (uint64_t)nt * kTileCells >= 0xffffffffull;
   const size_t per = (wide ? 8 : 4) * 2 + 4 * 2 + 8;
-  return (size_t)std::max<int64_t>(n, 1) * per + (size_t)nt * 8 + (1 << 20);
+  // Per unit (up to 4 per tile): start, colour list entry and range.
+  return (size_t)std::max<int64_t>(n, 1) * per + (size_t)nt * 4 * 24 + (1 << 20);
 }
 const double *assignor_totals(const Assignor *a) { return a->totals.as<double>(); }
 const unsigned long long *assignor_counts(const Assignor *a) {
