@@ -130,6 +130,25 @@ def test_mass_assign_matches_compiled_reference():
         assert ma.num_added == int(st[0])
 
 
+@pytest.mark.parametrize("cell", [3.450520833333333, 0.1, 7.0 / 3.0])
+def test_cell_faces_match_division(cell):
+    """Particles within a few ulps of cell faces land in the cells IEEE
+    division puts them in (the kernels divide through the reciprocal)."""
+    rng = np.random.default_rng(17)
+    shape = (16, 16, 16)
+    posmin = np.array([-123.456, 0.0, 987.654321])
+    n = 60000
+    pos = posmin + rng.integers(0, 17, size=(n, 3)) * cell
+    pos = pos + rng.integers(-3, 4, size=(n, 3)) * np.spacing(pos)
+    posw = np.concatenate([pos, np.ones((n, 1))], axis=1)
+    for periodic in (False, True):
+        g, ma = _assign_gpu(posw, shape, posmin, cell, 0, periodic)
+        ref, st = O.mass_assign(posw, shape, posmin, cell, 0, periodic)
+        assert np.array_equal(_device_grid_values(g), ref)
+        assert ma.num_added == int(st[0])
+        assert ma.num_skipped == int(st[1])
+
+
 def test_mass_assign_is_deterministic():
     shape = (64, 64, 64)
     posw = clustered_catalog(400000, [0, 0, 0], [640, 640, 640], 5, ncenters=200)
