@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "fc_common.cuh"
@@ -99,11 +100,13 @@ __device__ __forceinline__ bool dev_grid_coords(const double *p,
   return true;
 }
 
-// floor(x) as a cell index.  A wrapped coordinate can round up to exactly
-// n; that point is the upper edge of cell n-1, which is where it goes.
+// floor(x) as a cell index.  A periodically wrapped coordinate can round up
+// to exactly n, which is the periodic image of 0: cell 0 with offset 0, as
+// the reference's wrapped stencil indices place it.  Offsets within the cell
+// are x - floor(x).
 __device__ __forceinline__ int home_cell(double x, int n) {
   int i = (int)floor(x);
-  return i >= n ? n - 1 : (i < 0 ? 0 : i);
+  return i >= n ? i - n : (i < 0 ? 0 : i);
 }
 
 // 1-D stencil weights per scheme; the particle weight is folded into the x
@@ -322,13 +325,10 @@ __global__ void __launch_bounds__(kScatterThreads)
       const double *p = posw + 4 * (size_t)idx;
       double x[3];
       dev_grid_coords(p, g, x);
-      const int ix = home_cell(x[0], g.n[0]);
-      const int iy = home_cell(x[1], g.n[1]);
-      const int iz = home_cell(x[2], g.n[2]);
       pcell[threadIdx.x] = (int)(keys[c0 + threadIdx.x] & (kTileCells - 1));
       double *wt = wts + threadIdx.x * 3 * W;
-      Stencil<S>::weights(x[0] - ix, x[1] - iy, x[2] - iz, p[3], wt, wt + W,
-                          wt + 2 * W);
+      Stencil<S>::weights(x[0] - floor(x[0]), x[1] - floor(x[1]),
+                          x[2] - floor(x[2]), p[3], wt, wt + W, wt + 2 * W);
     }
     __syncthreads();
     for (int c = threadIdx.x; c <= kTileCells; c += blockDim.x) {
@@ -577,9 +577,9 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
         double *d = pd + 4 * i;
         double x[3];
         dev_grid_coords(d, g, x);
-        d[0] = x[0] - home_cell(x[0], g.n[0]);
-        d[1] = x[1] - home_cell(x[1], g.n[1]);
-        d[2] = x[2] - home_cell(x[2], g.n[2]);
+        d[0] = x[0] - floor(x[0]);
+        d[1] = x[1] - floor(x[1]);
+        d[2] = x[2] - floor(x[2]);
       }
       __syncthreads();  // also orders the zeroing of acc before round 0
       cstart[h] = lower_bound_smem(pc, m, h);
@@ -724,6 +724,7 @@ void scatter_p_kernel(int scheme, const void **fn, size_t *smem) {
 // MassAssignor state (mass_assignor.h:30-234) with a device-side buffer.
 struct Assignor {
   Grid *grid;
+  std::weak_ptr<int> grid_alive;
   int scheme;
   bool periodic;
   int64_t buffer_size;
@@ -764,7 +765,8 @@ struct Assignor {
   cudaStream_t stream_override = nullptr;
 
   Assignor(Grid *g, int scheme_, bool periodic_, int64_t buffer_size_)
-      : grid(g), scheme(scheme_), periodic(periodic_), buffer_size(buffer_size_) {
+      : grid(g), grid_alive(g->alive), scheme(scheme_), periodic(periodic_),
+        buffer_size(buffer_size_) {
     FC_REQUIRE(scheme >= 0 && scheme <= 3, FC_ERR_INVALID,
                "unknown distribution scheme");
     FC_REQUIRE(scheme != 2 || FC_HAVE_D12, FC_ERR_UNSUPPORTED,
@@ -820,7 +822,8 @@ struct Assignor {
   }
 
   ~Assignor() {
-    if (grid && grid->stream) cudaStreamSynchronize(grid->stream);
+    // The grid may have gone first (its destructor drains its stream).
+    if (!grid_alive.expired() && grid->stream) cudaStreamSynchronize(grid->stream);
   }
 
   cudaStream_t stream() const {

@@ -1,6 +1,7 @@
 // fc_internal.h -- objects behind the opaque C handles of fc_api.h.
 #pragma once
 
+#include <memory>
 #include <atomic>
 #include <vector>
 
@@ -26,6 +27,8 @@ struct Grid {
   cudaStream_t stream = nullptr;
   DeviceBuffer data;
   DeviceBuffer scratch;
+  // Expires with the grid, so objects that use it can tell it has gone.
+  std::shared_ptr<int> alive = std::make_shared<int>(0);
 
   Grid(const int shp[3], const double pmin[3], double cell);
   ~Grid();
