@@ -192,10 +192,14 @@ __global__ void k_cell_bins(const double *__restrict__ ax,
 }
 
 // Converts an FP64 complex grid to FP32 (set_grid2_fft in mixed precision).
-__global__ void k_z2c(const double2 *in, float2 *out, size_t n) {
+// rows of h complex values, written `pitch` elements apart.
+__global__ void k_z2c(const double2 *in, float2 *out, size_t n, int h,
+                      int pitch) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    out[i] = make_float2((float)in[i].x, (float)in[i].y);
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t row = i / h;
+    out[row * pitch + (i - row * h)] = make_float2((float)in[i].x, (float)in[i].y);
+  }
 }
 
 // ------------------------------------------------------------------ host
@@ -699,16 +703,19 @@ struct Correlator {
   void set_grid2_fft_host(const double *host_complex) {
     const size_t nc = geo.ncomplex();
     if (fused) {
+      const int h = fused->g.h, hp = fused->g.hp;
       if (fp64()) {
-        FC_CUDA(cudaMemcpyAsync(fused->g_data(), host_complex,
-                                nc * sizeof(double2), cudaMemcpyHostToDevice,
-                                stream));
+        FC_CUDA(cudaMemcpy2DAsync(fused->g_data(), hp * sizeof(double2),
+                                  host_complex, h * sizeof(double2),
+                                  h * sizeof(double2), nc / h,
+                                  cudaMemcpyHostToDevice, stream));
       } else {
         DeviceBuffer tmp(nc * sizeof(double2));
         FC_CUDA(cudaMemcpyAsync(tmp.get(), host_complex, nc * sizeof(double2),
                                 cudaMemcpyHostToDevice, stream));
         k_z2c<<<grid_for(nc, 256), 256, 0, stream>>>(
-            tmp.as<double2>(), static_cast<float2 *>(fused->g_data()), nc);
+            tmp.as<double2>(), static_cast<float2 *>(fused->g_data()), nc, h,
+            hp);
         FC_LAUNCH_CHECK();
         FC_CUDA(cudaStreamSynchronize(stream));
       }
@@ -724,8 +731,9 @@ struct Correlator {
       g2.resize(nc * sizeof(float2));
       FC_CUDA(cudaMemcpyAsync(tmp.get(), host_complex, nc * sizeof(double2),
                               cudaMemcpyHostToDevice, stream));
+      const int h = (int)(nc / ((size_t)geo.shape[0] * geo.shape[1]));
       k_z2c<<<grid_for(nc, 256), 256, 0, stream>>>(tmp.as<double2>(),
-                                                   g2.as<float2>(), nc);
+                                                   g2.as<float2>(), nc, h, h);
       FC_LAUNCH_CHECK();
       FC_CUDA(cudaStreamSynchronize(stream));
     }
@@ -1011,8 +1019,8 @@ size_t correlator_footprint(int kind, const int shape[3], double cell,
   const char *mode = std::getenv("FFTCORR_B200_FFT");
   const bool want_fused = !(mode && std::string(mode) == "cufft");
   if (kind == FC_SURVEY && want_fused && FusedSurvey::supported(g.shape, g.rsize)) {
-    const size_t h = g.shape[2] / 2 + 1;
-    bytes += 2 * g.ncomplex() * eb;                          // W, G
+    const size_t h = (g.shape[2] / 2 + 1 + 15) / 16 * 16;   // row pitch
+    bytes += 2 * (size_t)g.shape[0] * g.shape[1] * h * eb;   // W, G
     bytes += (size_t)g.rsize * g.shape[1] * h * eb;          // Wr
     bytes += (size_t)g.rsize * g.rsize * h * eb;             // Wry
     if (precision != FC_FP64)                                // FP32 density,

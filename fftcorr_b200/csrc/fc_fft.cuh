@@ -26,24 +26,27 @@ struct Vec2<double> {
   using type = double2;
 };
 
-// Arithmetic on float2 as a vector of two lanes (used by CPair below).
+// Arithmetic on float2 as a vector of two lanes (used by CPair below), in
+// the packed two-lane FP32 instructions of sm_100 (one issue for both
+// lanes; each lane rounds as the scalar operation does).
+__device__ __forceinline__ float2 f2splat(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float2 operator+(float2 a, float2 b) {
-  return make_float2(a.x + b.x, a.y + b.y);
+  return __fadd2_rn(a, b);
 }
 __device__ __forceinline__ float2 operator-(float2 a, float2 b) {
-  return make_float2(a.x - b.x, a.y - b.y);
+  return __ffma2_rn(b, f2splat(-1.f), a);  // b * -1 is exact
 }
 __device__ __forceinline__ float2 operator-(float2 a) {
   return make_float2(-a.x, -a.y);
 }
 __device__ __forceinline__ float2 operator*(float2 a, float s) {
-  return make_float2(a.x * s, a.y * s);
+  return __fmul2_rn(a, f2splat(s));
 }
 __device__ __forceinline__ float2 operator*(float s, float2 a) {
-  return make_float2(s * a.x, s * a.y);
+  return __fmul2_rn(f2splat(s), a);
 }
 __device__ __forceinline__ float2 operator*(float2 a, float2 b) {
-  return make_float2(a.x * b.x, a.y * b.y);  // lane by lane
+  return __fmul2_rn(a, b);  // lane by lane
 }
 
 // Two complex numbers of two independent transforms (columns or rows)
@@ -121,8 +124,8 @@ __device__ __forceinline__ C cconj(C a) {
 // A pair times one shared complex twiddle.
 __device__ __forceinline__ CPair cmul(CPair a, float2 w) {
   CPair r;
-  r.x = a.x * w.x - a.y * w.y;
-  r.y = a.x * w.y + a.y * w.x;
+  r.x = __ffma2_rn(a.y, f2splat(-w.y), __fmul2_rn(a.x, f2splat(w.x)));
+  r.y = __ffma2_rn(a.y, f2splat(w.x), __fmul2_rn(a.x, f2splat(w.y)));
   return r;
 }
 // (sign * i) * a

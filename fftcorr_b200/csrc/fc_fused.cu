@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     d = csub(a, c);
     o.x = (T)0.5 * d.y;  // -i (a - c) / 2
     o.y = (T)-0.5 * d.x;
-    W[row * g.h + k] = cadd(e, cmul(__ldg(&tabz[k]), o));
+    W[row * g.hp + k] = cadd(e, cmul(__ldg(&tabz[k]), o));
   }
 }
 
@@ -236,13 +236,13 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
   C *buf = reinterpret_cast<C *>(smem_raw);
   const int kz0 = blockIdx.x * B;
   const int x = blockIdx.y;
-  const int64_t base = (int64_t)x * g.n1 * g.h;
-  load_columns<B>(buf, W, base, g.h, g.n1, kz0, g.h);
+  const int64_t base = (int64_t)x * g.n1 * g.hp;
+  load_columns<B>(buf, W, base, g.hp, g.n1, kz0, g.h);
   buf = fft_columns<B>(buf, buf + g.n1 * BP, g.py, taby, -1);
   for (int idx = threadIdx.x; idx < g.n1 * B; idx += blockDim.x) {
     const int i = idx / B;
     const int b = idx - i * B;
-    if (kz0 + b < g.h) W[base + (int64_t)i * g.h + kz0 + b] = buf[i * BP + b];
+    if (kz0 + b < g.h) W[base + (int64_t)i * g.hp + kz0 + b] = buf[i * BP + b];
   }
 }
 
@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
   C *buf = reinterpret_cast<C *>(smem_raw);
   const int kz0 = blockIdx.x * B;
   const int yy = blockIdx.y;
-  const int64_t stride = (int64_t)g.n1 * g.h;
-  const int64_t base = (int64_t)yy * g.h;
+  const int64_t stride = (int64_t)g.n1 * g.hp;
+  const int64_t base = (int64_t)yy * g.hp;
   C *other = buf + g.n0 * BP;
   load_columns<B>(buf, W, base, stride, g.n0, kz0, g.h);
   {
@@ -314,8 +314,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
       __syncthreads();
     }
     buf = fft_columns<B>(buf, other, g.px, tabx, +1);
-    const int64_t obase = (int64_t)yy * g.h;
-    const int64_t ostride = (int64_t)g.n1 * g.h;
+    const int64_t obase = (int64_t)yy * g.hp;
+    const int64_t ostride = (int64_t)g.n1 * g.hp;
     for (int idx = threadIdx.x; idx < g.rs * B; idx += blockDim.x) {
       const int ri = idx / B;
       const int b = idx - ri * B;
@@ -338,16 +338,16 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
   C *buf = reinterpret_cast<C *>(smem_raw);
   const int kz0 = blockIdx.x * B;
   const int ri = blockIdx.y;
-  const int64_t base = (int64_t)ri * g.n1 * g.h;
-  load_columns<B>(buf, Wr, base, g.h, g.n1, kz0, g.h);
+  const int64_t base = (int64_t)ri * g.n1 * g.hp;
+  load_columns<B>(buf, Wr, base, g.hp, g.n1, kz0, g.h);
   buf = fft_columns<B>(buf, buf + g.n1 * BP, g.py, taby, +1);
-  const int64_t obase = (int64_t)ri * g.rs * g.h;
+  const int64_t obase = (int64_t)ri * g.rs * g.hp;
   for (int idx = threadIdx.x; idx < g.rs * B; idx += blockDim.x) {
     const int rj = idx / B;
     const int b = idx - rj * B;
     if (kz0 + b >= g.h) continue;
     const int y = ((rj - g.ro) % g.n1 + g.n1) % g.n1;
-    Wry[obase + (int64_t)rj * g.h + kz0 + b] = buf[y * BP + b];
+    Wry[obase + (int64_t)rj * g.hp + kz0 + b] = buf[y * BP + b];
   }
 }
 
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     z.x = 0;
     z.y = 0;
     if (row < nrows) {
-      const C *X = Wry + (int64_t)row * g.h;
+      const C *X = Wry + (int64_t)row * g.hp;
       C a = X[k];
       C c = cconj(X[M - k]);
       if (k == 0) {
@@ -451,20 +451,20 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const int b = threadIdx.x - t * Q::B;
   const int kz0 = blockIdx.x * Q::B;
   const bool valid = kz0 + b < g.h;
-  const int64_t base = (int64_t)blockIdx.y * L * g.h + kz0 + b;
+  const int64_t base = (int64_t)blockIdx.y * L * g.hp + kz0 + b;
   C v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     v[u].x = 0;
     v[u].y = 0;
-    if (valid) v[u] = W[base + (int64_t)(t + Q::TPC * u) * g.h];
+    if (valid) v[u] = W[base + (int64_t)(t + Q::TPC * u) * g.hp];
   }
   const int rb = Q::rd_base(t, b);
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; },
              [&](int u) { return &ex[Q::rd(rb, t, b, u)]; }, taby, -1);
   if (valid) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) W[base + (int64_t)(t + Q::TPC * u) * g.h] = v[u];
+    for (int u = 0; u < 8; ++u) W[base + (int64_t)(t + Q::TPC * u) * g.hp] = v[u];
   }
 }
 
@@ -481,24 +481,24 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const int kz0 = blockIdx.x * Q::B;
   const int ri = blockIdx.y;
   const bool valid = kz0 + b < g.h;
-  const int64_t base = (int64_t)ri * L * g.h + kz0 + b;
+  const int64_t base = (int64_t)ri * L * g.hp + kz0 + b;
   C v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     v[u].x = 0;
     v[u].y = 0;
-    if (valid) v[u] = Wr[base + (int64_t)(t + Q::TPC * u) * g.h];
+    if (valid) v[u] = Wr[base + (int64_t)(t + Q::TPC * u) * g.hp];
   }
   const int rb = Q::rd_base(t, b);
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::B + b]; },
              [&](int u) { return &ex[Q::rd(rb, t, b, u)]; }, taby, +1);
   if (!valid) return;
-  const int64_t obase = (int64_t)ri * g.rs * g.h + kz0 + b;
+  const int64_t obase = (int64_t)ri * g.rs * g.hp + kz0 + b;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
     for (int rj = (y + g.ro) % L; rj < g.rs; rj += L)
-      Wry[obase + (int64_t)rj * g.h] = v[u];
+      Wry[obase + (int64_t)rj * g.hp] = v[u];
   }
 }
 
@@ -517,8 +517,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const int yy = blockIdx.y;
   const int kzi = kz0 + b;
   const bool valid = kzi < g.h;
-  const int64_t stride = (int64_t)g.n1 * g.h;
-  const int64_t base = (int64_t)yy * g.h + kzi;
+  const int64_t stride = (int64_t)g.n1 * g.hp;
+  const int64_t base = (int64_t)yy * g.hp + kzi;
   auto exf = [&](int i) { return &ex[Q::row(i) * Q::B + b]; };
   C v[8];
   // In product mode the G column is loaded together with the W column, so
@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
     }
     reg_fft<L>(v, t, exf, exr, tabx, +1);
     if (valid) {
-      const int64_t obase = (int64_t)yy * g.h + kzi;
+      const int64_t obase = (int64_t)yy * g.hp + kzi;
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const int x = t + Q::TPC * u;
@@ -646,7 +646,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
   __syncthreads();
   if (!valid) return;
-  C *dst = W + row * g.h;
+  C *dst = W + row * g.hp;
   for (int k = t; k <= L; k += Q::TPC) {
     const C a = *exf(k == L ? 0 : k);
     const C c = cconj(*exf(k == 0 ? 0 : L - k));
@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   const int row = blockIdx.x * Q::B + b;
   const bool valid = row < nrows;
   C v[8];
-  const C *X = Wry + (int64_t)(valid ? row : 0) * g.h;
+  const C *X = Wry + (int64_t)(valid ? row : 0) * g.hp;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int k = t + Q::TPC * u;
@@ -755,12 +755,12 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   const int p = threadIdx.x - t * Q::PB;
   const int c0 = blockIdx.x * Q::B + p, c1 = c0 + Q::PB;
   const bool v0 = c0 < g.h, v1 = c1 < g.h;
-  const int64_t base = (int64_t)blockIdx.y * L * g.h;
+  const int64_t base = (int64_t)blockIdx.y * L * g.hp;
   const float2 zero = make_float2(0.f, 0.f);
   CPair v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
+    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.hp;
     v[u] = cpack(v0 ? W[r + c0] : zero, v1 ? W[r + c1] : zero);
   }
   const int rb = Q::rd_base(t, p);
@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
              [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, -1);
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
+    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.hp;
     if (v0) W[r + c0] = clane0(v[u]);
     if (v1) W[r + c1] = clane1(v[u]);
   }
@@ -786,24 +786,24 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   const int c0 = blockIdx.x * Q::B + p, c1 = c0 + Q::PB;
   const bool v0 = c0 < g.h, v1 = c1 < g.h;
   const int ri = blockIdx.y;
-  const int64_t base = (int64_t)ri * L * g.h;
+  const int64_t base = (int64_t)ri * L * g.hp;
   const float2 zero = make_float2(0.f, 0.f);
   CPair v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.h;
+    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.hp;
     v[u] = cpack(v0 ? Wr[r + c0] : zero, v1 ? Wr[r + c1] : zero);
   }
   const int rb = Q::rd_base(t, p);
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
              [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, +1);
-  const int64_t obase = (int64_t)ri * g.rs * g.h;
+  const int64_t obase = (int64_t)ri * g.rs * g.hp;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
     for (int rj = (y + g.ro) % L; rj < g.rs; rj += L) {
-      if (v0) Wry[obase + (int64_t)rj * g.h + c0] = clane0(v[u]);
-      if (v1) Wry[obase + (int64_t)rj * g.h + c1] = clane1(v[u]);
+      if (v0) Wry[obase + (int64_t)rj * g.hp + c0] = clane0(v[u]);
+      if (v1) Wry[obase + (int64_t)rj * g.hp + c1] = clane1(v[u]);
     }
   }
 }
@@ -864,8 +864,8 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
 #pragma unroll
   for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
   __syncthreads();
-  float2 *dst0 = W + row0 * g.h;
-  float2 *dst1 = W + row1 * g.h;
+  float2 *dst0 = W + row0 * g.hp;
+  float2 *dst1 = W + row1 * g.hp;
   // Unrolled so the twiddle loads of all outputs issue together.
 #pragma unroll
   for (int i = 0; i <= L / Q::TPC; ++i) {
@@ -1053,6 +1053,7 @@ FusedSurvey::FusedSurvey(const int shape[3], int rsize, const int kshape[3],
   g.n2 = shape[2];
   g.m = shape[2] / 2;
   g.h = g.m + 1;
+  g.hp = (g.h + 15) / 16 * 16;
   g.rs = rsize;
   g.ro = rsize / 2;
   g.ks0 = kshape[0];
@@ -1071,11 +1072,11 @@ FusedSurvey::FusedSurvey(const int shape[3], int rsize, const int kshape[3],
     upload(taby, root_table<float2>(g.n1));
     upload(tabz, root_table<float2>(g.n2));
   }
-  const size_t nc = (size_t)g.n0 * g.n1 * g.h;
+  const size_t nc = (size_t)g.n0 * g.n1 * g.hp;
   W.resize(nc * eb);
   G.resize(nc * eb);
-  Wr.resize((size_t)g.rs * g.n1 * g.h * eb);
-  Wry.resize((size_t)g.rs * g.rs * g.h * eb);
+  Wr.resize((size_t)g.rs * g.n1 * g.hp * eb);
+  Wry.resize((size_t)g.rs * g.rs * g.hp * eb);
   if (!fp64) {
     rho32.resize((size_t)g.n0 * g.n1 * g.n2 * sizeof(float));
     rowtab.resize((size_t)g.n0 * g.n1 * 2 * sizeof(float4));

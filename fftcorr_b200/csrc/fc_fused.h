@@ -15,6 +15,8 @@ struct FusedGeom {
   int n0, n1, n2;  // grid shape
   int m;           // N2 / 2: complex length of the z transform
   int h;           // N2 / 2 + 1: half-complex z extent
+  int hp;          // row pitch of W, G, Wr, Wry: h rounded up to 16, so
+                   // every 16-column group starts on a 128-byte line
   int rs, ro;      // r-subgrid edge and its centre offset (rs / 2)
   int ks0, ks1, ks2;  // k-subgrid shape
   FftPlan px, py, pz;
@@ -56,7 +58,8 @@ class FusedSurvey {
             double ncells, double *ksub, double *rsub, const double *raxis,
             const KAxes &ka, cudaStream_t s, PhaseHook *hook);
 
-  // G in the half-complex layout [N0][N1][N2/2+1] (FP64 or FP32 complex).
+  // G in the half-complex layout [N0][N1][N2/2+1] with rows g.hp elements
+  // apart (FP64 or FP32 complex).
   void *g_data() const { return G.get(); }
   bool fp64() const { return fp64_; }
 
