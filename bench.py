@@ -297,9 +297,9 @@ def kernel_profile(job, dD, nD, dR, nR):
 # --no-fp64 --no-cpu-baseline`; the pass kernels see the same grid as the
 # full workload (only the catalogs are smaller).  Summaries under profiles/.
 TRAFFIC_PER_LAUNCH_512 = {
-    "zfwd": 1035.25e6,
-    "yfwd": 1025.13e6,
-    "xcorr": 1326.52e6,
+    "zfwd": 1055.39e6,
+    "yfwd": 1064.94e6,
+    "xcorr": 1391.60e6,
 }
 
 
