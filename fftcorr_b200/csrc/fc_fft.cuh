@@ -69,6 +69,32 @@ __device__ __forceinline__ float2 clane1(const CPair &v) {
   return make_float2(v.x.y, v.y.y);
 }
 
+// The same pair with one-lane FP32 instructions (for kernels where the packed
+// forms measure slower).
+struct SF2 {
+  float x, y;
+};
+__device__ __forceinline__ SF2 operator+(SF2 a, SF2 b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ SF2 operator-(SF2 a, SF2 b) { return {a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ SF2 operator-(SF2 a) { return {-a.x, -a.y}; }
+__device__ __forceinline__ SF2 operator*(SF2 a, float s) { return {a.x * s, a.y * s}; }
+__device__ __forceinline__ SF2 operator*(float s, SF2 a) { return {s * a.x, s * a.y}; }
+struct __align__(16) CPairS {
+  SF2 x, y;
+};
+__device__ __forceinline__ CPairS cpack_s(float2 a, float2 b) {
+  CPairS r;
+  r.x = {a.x, b.x};
+  r.y = {a.y, b.y};
+  return r;
+}
+__device__ __forceinline__ float2 clane0(const CPairS &v) {
+  return make_float2(v.x.x, v.y.x);
+}
+__device__ __forceinline__ float2 clane1(const CPairS &v) {
+  return make_float2(v.x.y, v.y.y);
+}
+
 // Scalar type of a complex (or complex-pair) type.
 template <typename C>
 struct Real;
@@ -82,6 +108,10 @@ struct Real<double2> {
 };
 template <>
 struct Real<CPair> {
+  using type = float;
+};
+template <>
+struct Real<CPairS> {
   using type = float;
 };
 
@@ -126,6 +156,12 @@ __device__ __forceinline__ CPair cmul(CPair a, float2 w) {
   CPair r;
   r.x = __ffma2_rn(a.y, f2splat(-w.y), __fmul2_rn(a.x, f2splat(w.x)));
   r.y = __ffma2_rn(a.y, f2splat(w.x), __fmul2_rn(a.x, f2splat(w.y)));
+  return r;
+}
+__device__ __forceinline__ CPairS cmul(CPairS a, float2 w) {
+  CPairS r;
+  r.x = a.x * w.x - a.y * w.y;
+  r.y = a.x * w.y + a.y * w.x;
   return r;
 }
 // (sign * i) * a

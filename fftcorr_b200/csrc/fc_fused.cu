@@ -819,7 +819,7 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   using Q = PP<L>;
   constexpr int RP = L + L / 8 + 1;
   extern __shared__ unsigned char smem_raw[];
-  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  CPairS *ex = reinterpret_cast<CPairS *>(smem_raw);
   const int pb = threadIdx.x / Q::TPC;
   const int t = threadIdx.x - pb * Q::TPC;
   const int64_t nrows = (int64_t)g.n0 * g.n1;
@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
     zt = (float)(z0 + (2 * t) * 1.0);
   }
   const float2 zero = make_float2(0.f, 0.f);
-  CPair v[8];
+  CPairS v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int jj = t + Q::TPC * u;
@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
       b.x = row_weight(rp1, b.x, zu);
       b.y = row_weight(rp1, b.y, zu + 1.0f);
     }
-    v[u] = cpack(a, b);
+    v[u] = cpack_s(a, b);
   }
   auto exf = [&](int i) { return &ex[pb * RP + i + (i >> 3)]; };
   reg_fft<L>(v, t, exf, tabz, -1, 2);
@@ -871,15 +871,15 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   for (int i = 0; i <= L / Q::TPC; ++i) {
     const int k = t + Q::TPC * i;
     if (k > L) break;
-    const CPair a = *exf(k == L ? 0 : k);
-    const CPair c = cconj(*exf(k == 0 ? 0 : L - k));
-    CPair e, o;
+    const CPairS a = *exf(k == L ? 0 : k);
+    const CPairS c = cconj(*exf(k == 0 ? 0 : L - k));
+    CPairS e, o;
     e.x = 0.5f * (a.x + c.x);
     e.y = 0.5f * (a.y + c.y);
-    const CPair d = csub(a, c);
+    const CPairS d = csub(a, c);
     o.x = 0.5f * d.y;
     o.y = -0.5f * d.x;
-    const CPair r = cadd(e, cmul(o, __ldg(&tabz[k])));
+    const CPairS r = cadd(e, cmul(o, __ldg(&tabz[k])));
     if (v0) dst0[k] = clane0(r);
     if (v1) dst1[k] = clane1(r);
   }
