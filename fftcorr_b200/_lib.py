@@ -185,6 +185,8 @@ _SIGNATURES = {
     "fc_corr_autocorrelate_grid_async": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "fc_corr_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_corr_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "fc_corr_set_term_shard": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
+                                              ctypes.c_int]),
     "fc_corr_profile": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(KernelTime),
                                        ctypes.c_int, c_int_p]),
     "fc_sum_sumsq_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_double_p,

@@ -133,6 +133,11 @@ class BaseCorrelator:
         res = self.results()
         return self._power_spectrum(res, squeeze), self._correlation(res, squeeze)
 
+    def set_term_shard(self, rank, world):
+        """Compute only the (ell, m) terms i with i % world == rank (survey
+        correlators); see fftcorr_b200.correlate.sharded."""
+        _lib.call("fc_corr_set_term_shard", self._handle, int(rank), int(world))
+
     # -------------------------------------------------------------- inputs
     def _host_grid(self, grid):
         grid = np.ascontiguousarray(grid, dtype=np.float64)

@@ -408,6 +408,10 @@ struct Correlator {
   cudaEvent_t ev_fft0 = nullptr, ev_fft1 = nullptr;
   double last_total = 0.0;
   int n_fft = 0;
+  // Survey (ell, m) terms this correlator computes: term i of the loop order
+  // (ell ascending, then m ascending) when i % term_world == term_rank.
+  int term_rank = 0, term_world = 1;
+  bool owns_term(int i) const { return i % term_world == term_rank; }
   // Launch shapes of the grid-stride kernels; results do not depend on them
   // (every cell is computed independently), so the autotuner may change them.
   LaunchShape ls_abs2{256, 8}, ls_ksub{256, 8}, ls_rsub{256, 8};
@@ -838,9 +842,11 @@ struct Correlator {
           prepared ? fused->input(rho) : fused->prepare_input(rho, stream);
       ProfHook hook(&prof, stream);
       const KAxes ka = kaxes();
+      int term = 0;
       for (int ell = 0; ell <= maxell; ell += 2) {
         zero_sub(true, true);
         for (int m = -ell; m <= ell; ++m) {
+          if (!owns_term(term++)) continue;
           fused->term(in, ell, m, xyz0, (double)ncells, ksub.as<double>(),
                       rsub.as<double>(), d_raxis.as<double>(), ka, stream,
                       prof.on ? &hook : nullptr);
@@ -851,9 +857,11 @@ struct Correlator {
       }
       return;
     }
+    int term = 0;
     for (int ell = 0; ell <= maxell; ell += 2) {
       zero_sub(true, true);
       for (int m = -ell; m <= ell; ++m) {
+        if (!owns_term(term++)) continue;
         weight<T>(rho, ell, m, 0.0);
         exec_r2c(work.get(), work.get());
         conj_mul<T>(false);
@@ -1214,6 +1222,19 @@ int fc_corr_footprint(int kind, const int shape[3], double cell_size,
     FC_REQUIRE(shape && bytes, FC_ERR_INVALID, "null argument");
     *bytes = correlator_footprint(kind, shape, cell_size, rmax, kmax, maxell,
                                   precision);
+  });
+}
+
+int fc_corr_set_term_shard(fc_correlator *corr, int rank, int world) {
+  return guard([&] {
+    Correlator *c = as_corr(corr);
+    FC_REQUIRE(world >= 1 && rank >= 0 && rank < world, FC_ERR_INVALID,
+               "term shard needs 0 <= rank < world");
+    FC_REQUIRE(world == 1 || c->kind == FC_SURVEY, FC_ERR_UNSUPPORTED,
+               "only the survey correlator has per-(ell, m) transforms to shard");
+    FC_CUDA(cudaStreamSynchronize(c->stream));
+    c->term_rank = rank;
+    c->term_world = world;
   });
 }
 

@@ -222,6 +222,14 @@ typedef struct fc_kernel_time {
   double seconds;  /* summed device time of those launches */
 } fc_kernel_time;
 int fc_corr_set_profiling(fc_correlator *corr, int enable);
+/* Splits a survey correlation's (ell, m) terms (the loop of
+ * correlator.h:421-489) over `world` ranks: this correlator computes term i
+ * (ell ascending, then m) when i % world == rank, and its histograms and
+ * zero lag are that share.  The histograms are linear in the terms, so the
+ * sum over ranks is the full result; bin counts are the same on every rank.
+ * world 1 (the default) computes every term.  FC_ERR_UNSUPPORTED for a
+ * periodic correlator with world > 1. */
+int fc_corr_set_term_shard(fc_correlator *corr, int rank, int world);
 /* Copies up to max entries; *n receives the number of kernel families. */
 int fc_corr_profile(fc_correlator *corr, fc_kernel_time *out, int max, int *n);
 

@@ -429,10 +429,12 @@ def periodic_correlate(grid, cell, window, rmax, dr, kmax, dk, maxell,
 
 
 def survey_correlate(grid, cell, posmin, window, rmax, dr, kmax, dk, maxell,
-                     grid2=None):
+                     grid2=None, terms=None):
     """Correlator (survey, Ylm about the observer) (correlator.h:381-497).
 
     grid2 None is autocorrelate(grid); otherwise cross_correlate(grid, grid2).
+    terms, if given, is the set of (ell, m) loop indices to include (the
+    others contribute nothing), for checking a term-sharded correlation.
     """
     grid = np.asarray(grid, dtype=np.float64)
     geo = Geometry(grid.shape, cell, window, rmax, dr, kmax, dk, maxell)
@@ -444,10 +446,14 @@ def survey_correlate(grid, cell, posmin, window, rmax, dr, kmax, dk, maxell,
     yc = sequence(0.5 - obs[1], 1.0, grid.shape[1])
     zc = sequence(0.5 - obs[2], 1.0, grid.shape[2])
     zerolag = None
+    term = -1
     for ell in range(0, maxell + 1, 2):
         rsub = np.zeros(geo.rshape)
         ksub = np.zeros(geo.kshape)
         for m in range(-ell, ell + 1):
+            term += 1
+            if terms is not None and term not in terms:
+                continue
             work = _rfftn(make_ylm(ell, m, xc, yc, zc, 1.0, grid))
             work *= g2c
             kylm = make_ylm(ell, m, geo.kx, geo.ky, geo.kz, 4.0 * math.pi,

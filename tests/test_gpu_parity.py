@@ -424,3 +424,49 @@ def test_golden_tables_through_gpu(hemi, golden_catalogs, golden_tables, fft_pat
         gold = golden_tables[f"{hemi}_{name}"]
         np.testing.assert_array_equal(tab[:, 2], gold[:, 2])
         np.testing.assert_allclose(tab, gold, rtol=1e-7)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_term_shards_sum_to_the_full_correlation(precision, fft_path):
+    """(ell, m) terms split over 3 ranks, run one after another on this GPU:
+    each share matches the oracle's share of the same terms, and the shares
+    sum to the unsharded correlation."""
+    from fftcorr_b200.correlate.sharded import owned_terms
+    shape, cell = (32, 32, 32), 12.0
+    posmin = np.array([-100.0, 250.0, -300.0])
+    nn, _ = _survey_field(shape, cell, posmin, 71)
+    args = (cell, posmin, TSC_ALIASED_CORRECTION, 70.0, 10.0, 0.12, 0.02, 4)
+    c = fb.Correlator(shape, *args, precision=precision)
+    c.autocorrelate(nn)
+    full = c.results()
+    tot = {"rhist": 0.0, "khist": 0.0, "zerolag": 0.0}
+    for rank in range(3):
+        c.set_term_shard(rank, 3)
+        c.autocorrelate(nn)
+        part = c.results()
+        np.testing.assert_array_equal(part["rcounts"], full["rcounts"])
+        np.testing.assert_array_equal(part["kcounts"], full["kcounts"])
+        if precision == "fp64":
+            terms = {i for i, _, _ in owned_terms(4, rank, 3)}
+            ref = O.survey_correlate(nn, *args, terms=terms)
+            _compare_results(part, ref, FP64_RTOL, f"shard {rank}")
+        for k in tot:
+            tot[k] = tot[k] + part[k]
+    for k in ("rhist", "khist"):
+        scale = np.max(np.abs(full[k]))
+        assert np.max(np.abs(tot[k] - full[k])) <= 1e-12 * scale
+    assert abs(tot["zerolag"] - full["zerolag"]) <= 1e-12 * abs(full["zerolag"])
+    c.set_term_shard(0, 1)
+    c.autocorrelate(nn)
+    assert np.array_equal(c.results()["rhist"], full["rhist"])
+
+
+def test_term_shard_arguments():
+    c = fb.Correlator((16, 16, 16), 10.0, np.array([-80.0, 5.0, 5.0]), 0, 30.0,
+                      5.0, 0.2, 0.05, 2)
+    with pytest.raises(ValueError):
+        c.set_term_shard(2, 2)
+    p = fb.PeriodicCorrelator((16, 16, 16), 10.0, 0, 30.0, 5.0, 0.2, 0.05, 2)
+    with pytest.raises(_lib.FcError):
+        p.set_term_shard(0, 2)
+    p.set_term_shard(0, 1)
