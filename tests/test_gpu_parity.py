@@ -317,6 +317,14 @@ def test_cross_correlations(fft_path):
     s.set_grid2(b)
     s.cross_correlate(a)
     _compare_results(s.results(), sref, FP64_RTOL, "survey-cross")
+    # The survey correlator takes a host FFT of grid2 too (rows padded on
+    # the device in the fused path).
+    for precision in ("fp64", "fp32"):
+        s2 = fb.Correlator(shape, *sargs, precision=precision)
+        s2.set_grid2_fft(np.fft.rfftn(b))
+        s2.cross_correlate(a)
+        _compare_results(s2.results(), sref, FP64_RTOL, "survey-cross-fft",
+                         fp32=precision == "fp32")
 
 
 @pytest.mark.parametrize("shape", [(20, 28, 30), (24, 18, 50), (16, 16, 33),
