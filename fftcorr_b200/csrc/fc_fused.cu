@@ -716,10 +716,12 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
 }
 
 // ------------------------------------------------- FP32 two-per-thread
-// FP32 y and z passes with two independent transforms per thread (CPair):
-// the same B columns (or rows) per CTA as the kernels above with half the
-// threads.  The two transforms share every twiddle load and index
-// computation and the shared-memory exchanges move 16 bytes per access.
+// FP32 y and z passes with two independent transforms per thread: the same
+// B columns (or rows) per CTA as the kernels above with half the threads.
+// The two transforms share every twiddle load and index computation and the
+// shared-memory exchanges move 16 bytes per access.  The y passes carry the
+// pair as CPair (packed two-lane instructions), the z pass as CPairS
+// (one-lane instructions), whichever measured faster for the pass.
 // Thread (t, p) holds columns p and p + PB of the CTA's B, so each global
 // access of a warp stays contiguous per row.  (The x pass keeps one column
 // per thread: with its second input stream and inverse transform, two
