@@ -320,6 +320,8 @@ def algorithmic_bytes(family, w, precision, rs, ks):
       yfwd   W in and out (2 Nc e)
       xcorr  W and G in (2 Nc e) + x-pruned Wr out (rs N1 h e)
              + k-subgrid weight read and read-modify-write (K0 K1 K2 * 24)
+      xcorr00  the ell = 0 term of an autocorrelation: G in (Nc e) + Wr out
+             + k-subgrid as xcorr (its transform is a multiple of G)
       yinv   Wr in (rs N1 h e) + Wry out (rs rs h e)
       zinv   Wry in (rs rs h e) + r-subgrid read-modify-write (rs^3 * 16)"""
     s = 8 if precision == "fp64" else 4
@@ -333,6 +335,7 @@ def algorithmic_bytes(family, w, precision, rs, ks):
         "zfwd": n * s + nc * e,
         "yfwd": 2 * nc * e,
         "xcorr": 2 * nc * e + rs * n1 * h * e + kc * 24,
+        "xcorr00": nc * e + rs * n1 * h * e + kc * 24,
         "yinv": rs * n1 * h * e + rs * rs * h * e,
         "zinv": rs * rs * h * e + rs ** 3 * 16,
         "weight": n * 8 + n * s,

@@ -849,7 +849,7 @@ struct Correlator {
           if (!owns_term(term++)) continue;
           fused->term(in, ell, m, xyz0, (double)ncells, ksub.as<double>(),
                       rsub.as<double>(), d_raxis.as<double>(), ka, stream,
-                      prof.on ? &hook : nullptr);
+                      prof.on ? &hook : nullptr, prepared);
           n_fft += 2;  // one forward and one (pruned) inverse transform
         }
         hist_rows(ell, true, true);

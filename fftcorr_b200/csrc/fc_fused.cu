@@ -506,7 +506,8 @@ template <typename T, int L, int MODE>
 __global__ void __launch_bounds__(P2<T, L>::THREADS)
     k_xcorr_p2(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
                C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
-               const C2<T> *__restrict__ tabx, const double *__restrict__ ktab) {
+               const C2<T> *__restrict__ tabx, const double *__restrict__ ktab,
+               T w00) {
   using C = C2<T>;
   using Q = P2<T, L>;
   extern __shared__ unsigned char smem_raw[];
@@ -523,14 +524,29 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   C v[8];
   // In product mode the G column is loaded together with the W column, so
   // both streams are in flight during the forward transform.
-  C gv[MODE == 0 ? 1 : 8];
+  C gv[MODE == 1 ? 8 : 1];
+  if constexpr (MODE == 2) {
+    // ell = 0 of an autocorrelation: the weighted field is w00 * rho, whose
+    // transform is w00 * G, so the product is w00 |G|^2 and neither W nor a
+    // forward transform is needed.
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    v[u].x = 0;
-    v[u].y = 0;
-    if (valid) v[u] = W[base + (t + Q::TPC * u) * stride];
+    for (int u = 0; u < 8; ++u) {
+      C gg;
+      gg.x = 0;
+      gg.y = 0;
+      if (valid) gg = G[base + (t + Q::TPC * u) * stride];
+      v[u].x = w00 * (gg.x * gg.x + gg.y * gg.y);
+      v[u].y = 0;
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      v[u].x = 0;
+      v[u].y = 0;
+      if (valid) v[u] = W[base + (t + Q::TPC * u) * stride];
+    }
   }
-  if constexpr (MODE != 0) {
+  if constexpr (MODE == 1) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       gv[u].x = 0;
@@ -540,15 +556,17 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   }
   const int rb = Q::rd_base(t, b);
   auto exr = [&](int u) { return &ex[Q::rd(rb, t, b, u)]; };
-  reg_fft<L>(v, t, exf, exr, tabx, -1);
+  if constexpr (MODE != 2) reg_fft<L>(v, t, exf, exr, tabx, -1);
   if constexpr (MODE == 0) {
     if (valid) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) out[base + (t + Q::TPC * u) * stride] = v[u];
     }
   } else {
+    if constexpr (MODE == 1) {
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = cmulc(v[u], gv[u]);
+      for (int u = 0; u < 8; ++u) v[u] = cmulc(v[u], gv[u]);
+    }
     // k-subgrid extraction (see k_xcorr): needs P at arbitrary rows.
     const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
     if (ksub != nullptr && kz0 <= oz) {
@@ -1012,6 +1030,8 @@ void p2_set_limits() {
                                cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   FC_CUDA(cudaFuncSetAttribute(k_xcorr_p2<T, L, 1>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  FC_CUDA(cudaFuncSetAttribute(k_xcorr_p2<T, L, 2>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   FC_CUDA(cudaFuncSetAttribute(k_zfwd_p2<T, L, true>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   FC_CUDA(cudaFuncSetAttribute(k_zfwd_p2<T, L, false>,
@@ -1228,11 +1248,11 @@ void FusedSurvey::xcorr(bool product, double *ksub, const double *ktab,
       if (!product)
         k_xcorr_p2<T, L, 0><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
-            nullptr);
+            nullptr, T(0));
       else
         k_xcorr_p2<T, L, 1><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g,
-            tabx.as<C2<T>>(), ktab);
+            tabx.as<C2<T>>(), ktab, T(0));
     });
     FC_LAUNCH_CHECK();
     return;
@@ -1250,6 +1270,19 @@ void FusedSurvey::xcorr(bool product, double *ksub, const double *ktab,
         W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g, tabx.as<C2<T>>(),
         ktab);
   }
+  FC_LAUNCH_CHECK();
+}
+
+template <typename T>
+void FusedSurvey::xcorr00(double *ksub, const double *ktab, double w00,
+                          cudaStream_t s) {
+  with_p2(g.n0, [&]<int L>() {
+    using Q = P2<T, L>;
+    dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
+    k_xcorr_p2<T, L, 2><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+        nullptr, G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g, tabx.as<C2<T>>(), ktab,
+        (T)w00);
+  });
   FC_LAUNCH_CHECK();
 }
 
@@ -1331,21 +1364,29 @@ void FusedSurvey::grid2(const void *rho_in, cudaStream_t s, const KAxes &ka) {
 void FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
                        double ncells, double *ksub, double *rsub,
                        const double *raxis, const KAxes &ka, cudaStream_t s,
-                       PhaseHook *hook) {
+                       PhaseHook *hook, bool g_of_input) {
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
   const double *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
   auto run = [&](auto tag) {
     using T = decltype(tag);
-    if (hook) hook->begin("zfwd");
-    zfwd<T>(rho_in, true, pw, xyz0, s);
-    if (hook) hook->end();
-    if (hook) hook->begin("yfwd");
-    yfwd<T>(s);
-    if (hook) hook->end();
-    if (hook) hook->begin("xcorr");
-    xcorr<T>(true, ksub, ktab, s);
-    if (hook) hook->end();
+    if (ell == 0 && g_of_input && is_p2(g.n0)) {
+      // The weight is the constant pw.value0, so the term's transform is
+      // value0 * G (see k_xcorr_p2, MODE 2).
+      if (hook) hook->begin("xcorr00");
+      xcorr00<T>(ksub, ktab, pw.value0, s);
+      if (hook) hook->end();
+    } else {
+      if (hook) hook->begin("zfwd");
+      zfwd<T>(rho_in, true, pw, xyz0, s);
+      if (hook) hook->end();
+      if (hook) hook->begin("yfwd");
+      yfwd<T>(s);
+      if (hook) hook->end();
+      if (hook) hook->begin("xcorr");
+      xcorr<T>(true, ksub, ktab, s);
+      if (hook) hook->end();
+    }
     if (hook) hook->begin("yinv");
     yinv<T>(s);
     if (hook) hook->end();

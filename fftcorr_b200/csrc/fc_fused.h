@@ -56,7 +56,8 @@ class FusedSurvey {
   // the FP64 subgrids.
   void term(const void *rho_in, int ell, int m, const double xyz0[3],
             double ncells, double *ksub, double *rsub, const double *raxis,
-            const KAxes &ka, cudaStream_t s, PhaseHook *hook);
+            const KAxes &ka, cudaStream_t s, PhaseHook *hook,
+            bool g_of_input = false);
 
   // G in the half-complex layout [N0][N1][N2/2+1] with rows g.hp elements
   // apart (FP64 or FP32 complex).
@@ -77,6 +78,8 @@ class FusedSurvey {
   void yfwd(cudaStream_t s);
   template <typename T>
   void xcorr(bool product, double *ksub, const double *ktab, cudaStream_t s);
+  template <typename T>
+  void xcorr00(double *ksub, const double *ktab, double w00, cudaStream_t s);
   // Weights of the k-subgrid cells for (ell, m), built on first use.
   const double *k_table(int ell, int m, const KAxes &ka, cudaStream_t s);
   template <typename T>
