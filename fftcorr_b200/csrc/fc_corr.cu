@@ -847,10 +847,12 @@ struct Correlator {
         zero_sub(true, true);
         for (int m = -ell; m <= ell; ++m) {
           if (!owns_term(term++)) continue;
-          fused->term(in, ell, m, xyz0, (double)ncells, ksub.as<double>(),
-                      rsub.as<double>(), d_raxis.as<double>(), ka, stream,
-                      prof.on ? &hook : nullptr, prepared);
-          n_fft += 2;  // one forward and one (pruned) inverse transform
+          // One forward and one (pruned) inverse transform, or the inverse
+          // alone for the ell = 0 term of an autocorrelation.
+          n_fft += fused->term(in, ell, m, xyz0, (double)ncells,
+                               ksub.as<double>(), rsub.as<double>(),
+                               d_raxis.as<double>(), ka, stream,
+                               prof.on ? &hook : nullptr, prepared);
         }
         hist_rows(ell, true, true);
         if (ell == 0) save_zerolag();

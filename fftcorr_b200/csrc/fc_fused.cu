@@ -1361,16 +1361,17 @@ void FusedSurvey::grid2(const void *rho_in, cudaStream_t s, const KAxes &ka) {
   }
 }
 
-void FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
+int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
                        double ncells, double *ksub, double *rsub,
                        const double *raxis, const KAxes &ka, cudaStream_t s,
                        PhaseHook *hook, bool g_of_input) {
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
   const double *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
+  const bool from_g = ell == 0 && g_of_input && is_p2(g.n0);
   auto run = [&](auto tag) {
     using T = decltype(tag);
-    if (ell == 0 && g_of_input && is_p2(g.n0)) {
+    if (from_g) {
       // The weight is the constant pw.value0, so the term's transform is
       // value0 * G (see k_xcorr_p2, MODE 2).
       if (hook) hook->begin("xcorr00");
@@ -1398,6 +1399,7 @@ void FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
     run(double());
   else
     run(float());
+  return from_g ? 1 : 2;
 }
 
 }  // namespace fc

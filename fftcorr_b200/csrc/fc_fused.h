@@ -54,7 +54,8 @@ class FusedSurvey {
   void grid2(const void *rho_in, cudaStream_t s, const KAxes &ka);
   // One (ell, m) term of Correlator::correlate_internal, accumulated into
   // the FP64 subgrids.
-  void term(const void *rho_in, int ell, int m, const double xyz0[3],
+  // Returns the number of full-grid transforms run (1 or 2).
+  int term(const void *rho_in, int ell, int m, const double xyz0[3],
             double ncells, double *ksub, double *rsub, const double *raxis,
             const KAxes &ka, cudaStream_t s, PhaseHook *hook,
             bool g_of_input = false);
