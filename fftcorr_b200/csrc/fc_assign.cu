@@ -581,7 +581,7 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
         d[1] = x[1] - floor(x[1]);
         d[2] = x[2] - floor(x[2]);
       }
-      __syncthreads();  // also orders the zeroing of acc before round 0
+      __syncthreads();  // also orders the zeroing of acc before the first offset
       cstart[h] = lower_bound_smem(pc, m, h);
       if (h == 0) cstart[T] = m;
       __syncthreads();
