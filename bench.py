@@ -323,7 +323,8 @@ def algorithmic_bytes(family, w, precision, rs, ks):
       xcorr00  the ell = 0 term of an autocorrelation: G in (Nc e) + Wr out
              + k-subgrid as xcorr (its transform is a multiple of G)
       yinv   Wr in (rs N1 h e) + Wry out (rs rs h e)
-      zinv   Wry in (rs rs h e) + r-subgrid read-modify-write (rs^3 * 16)"""
+      zinv   Wry in (rs rs h e) + r-subgrid weight read and
+             read-modify-write (rs^3 * 24)"""
     s = 8 if precision == "fp64" else 4
     e = 2 * s
     n0, n1, n2 = w.ngrid
@@ -337,7 +338,7 @@ def algorithmic_bytes(family, w, precision, rs, ks):
         "xcorr": 2 * nc * e + rs * n1 * h * e + kc * 24,
         "xcorr00": nc * e + rs * n1 * h * e + kc * 24,
         "yinv": rs * n1 * h * e + rs * rs * h * e,
-        "zinv": rs * rs * h * e + rs ** 3 * 16,
+        "zinv": rs * rs * h * e + rs ** 3 * 24,
         "weight": n * 8 + n * s,
         "copy_pad": n * 8 + n * s,
         "conj_mul": 3 * nc * e,

@@ -359,7 +359,7 @@ template <typename T>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     k_zinv_rsub(const C2<T> *__restrict__ Wry, double *__restrict__ rsub,
                 FusedGeom g, const C2<T> *__restrict__ tabz,
-                const double *__restrict__ raxis, YlmParams pr) {
+                const double *__restrict__ rtab) {
   using C = C2<T>;
   constexpr int B = Tile<T>::B;
   constexpr int BP = B + 1;
@@ -403,8 +403,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     const int z = ((rk - g.ro) % g.n2 + g.n2) % g.n2;
     const C zz = buf[(z >> 1) * BP + b];
     const double v = (double)((z & 1) ? zz.y : zz.x);
-    const double yv = ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
-    rsub[(size_t)row * g.rs + rk] += yv * v;
+    const size_t cell = (size_t)row * g.rs + rk;
+    rsub[cell] += rtab[cell] * v;
   }
 }
 
@@ -682,7 +682,7 @@ template <typename T, int L>
 __global__ void __launch_bounds__(P2<T, L>::THREADS)
     k_zinv_p2(const C2<T> *__restrict__ Wry, double *__restrict__ rsub,
               FusedGeom g, const C2<T> *__restrict__ tabz,
-              const double *__restrict__ raxis, YlmParams pr) {
+              const double *__restrict__ rtab) {
   using C = C2<T>;
   using Q = P2<T, L>;
   constexpr int RP = L + L / 8 + 1;
@@ -726,8 +726,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
       const int z = 2 * jj + h;
       const double val = (double)(h ? v[u].y : v[u].x);
       for (int rk = (z + g.ro) % g.n2; rk < g.rs; rk += g.n2) {
-        const double yv = ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
-        rsub[(size_t)row * g.rs + rk] += yv * val;
+        const size_t cell = (size_t)row * g.rs + rk;
+        rsub[cell] += rtab[cell] * val;
       }
     }
   }
@@ -916,6 +916,21 @@ __global__ void k_rowpoly(float4 *__restrict__ tab, int64_t nrows, int n1,
     const RowPoly r = row_poly(p, x0 + x * 1.0, y0 + y * 1.0);
     tab[2 * row] = make_float4(r.c[0], r.c[1], r.c[2], r.c[3]);
     tab[2 * row + 1] = make_float4(r.c[4], r.rxy2, 0.f, 0.f);
+  }
+}
+
+// Per-cell r-subgrid weight of one (ell, m): Y_lm(r) with the r-subgrid
+// normalisation (make_ylm, correlator.h:477-480), computed once per
+// correlator and multipole so the z inverse pass does a multiply-add.
+__global__ void k_rtable(double *__restrict__ tab, int rs,
+                         const double *__restrict__ raxis, YlmParams pr) {
+  const size_t n = (size_t)rs * rs * rs;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int rk = (int)(i % rs);
+    const int rj = (int)((i / rs) % rs);
+    const int ri = (int)(i / ((size_t)rs * rs));
+    tab[i] = ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
   }
 }
 
@@ -1310,15 +1325,14 @@ void FusedSurvey::yinv(cudaStream_t s) {
 }
 
 template <typename T>
-void FusedSurvey::zinv(double *rsub, const double *raxis, const YlmParams &pr,
-                       cudaStream_t s) {
+void FusedSurvey::zinv(double *rsub, const double *rtab, cudaStream_t s) {
   if (is_p2(g.m)) {
     with_p2(g.m, [&]<int L>() {
       using Q = P2<T, L>;
       const int nrows = g.rs * g.rs;
       const unsigned blocks = (unsigned)((nrows + Q::B - 1) / Q::B);
       k_zinv_p2<T, L><<<blocks, Q::THREADS, p2_row_smem<T, L>(), s>>>(
-          Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), raxis, pr);
+          Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), rtab);
     });
     FC_LAUNCH_CHECK();
     return;
@@ -1327,8 +1341,21 @@ void FusedSurvey::zinv(double *rsub, const double *raxis, const YlmParams &pr,
   const int nrows = g.rs * g.rs;
   const unsigned blocks = (unsigned)((nrows + B - 1) / B);
   k_zinv_rsub<T><<<blocks, threads_for(g.m, B), smem(g.m), s>>>(
-      Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), raxis, pr);
+      Wry.as<C2<T>>(), rsub, g, tabz.as<C2<T>>(), rtab);
   FC_LAUNCH_CHECK();
+}
+
+const double *FusedSurvey::r_table(int ell, int m, const double *raxis,
+                                   const YlmParams &pr, cudaStream_t s) {
+  const int key = ell * 16 + (m + ell);
+  auto it = rtabs.find(key);
+  if (it != rtabs.end()) return it->second.as<double>();
+  const size_t n = (size_t)g.rs * g.rs * g.rs;
+  DeviceBuffer &b = rtabs[key];
+  b.resize(std::max<size_t>(n, 1) * sizeof(double));
+  k_rtable<<<grid_for(n, 256), 256, 0, s>>>(b.as<double>(), g.rs, raxis, pr);
+  FC_LAUNCH_CHECK();
+  return b.as<double>();
 }
 
 const double *FusedSurvey::k_table(int ell, int m, const KAxes &ka,
@@ -1368,6 +1395,7 @@ int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
   const double *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
+  const double *rtab = r_table(ell, m, raxis, pr, s);
   const bool from_g = ell == 0 && g_of_input && is_p2(g.n0);
   auto run = [&](auto tag) {
     using T = decltype(tag);
@@ -1392,7 +1420,7 @@ int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
     yinv<T>(s);
     if (hook) hook->end();
     if (hook) hook->begin("zinv");
-    zinv<T>(rsub, raxis, pr, s);
+    zinv<T>(rsub, rtab, s);
     if (hook) hook->end();
   };
   if (fp64_)

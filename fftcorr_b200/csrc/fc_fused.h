@@ -83,16 +83,19 @@ class FusedSurvey {
   void xcorr00(double *ksub, const double *ktab, double w00, cudaStream_t s);
   // Weights of the k-subgrid cells for (ell, m), built on first use.
   const double *k_table(int ell, int m, const KAxes &ka, cudaStream_t s);
+  // Y_lm(r) of the r-subgrid cells for (ell, m), built on first use.
+  const double *r_table(int ell, int m, const double *raxis,
+                        const YlmParams &pr, cudaStream_t s);
   template <typename T>
   void yinv(cudaStream_t s);
   template <typename T>
-  void zinv(double *rsub, const double *raxis, const YlmParams &pr,
-            cudaStream_t s);
+  void zinv(double *rsub, const double *rtab, cudaStream_t s);
 
   bool fp64_;
   DeviceBuffer tabx, taby, tabz;
   DeviceBuffer W, G, Wr, Wry, rho32;
   std::map<int, DeviceBuffer> ktabs;
+  std::map<int, DeviceBuffer> rtabs;
   DeviceBuffer rowtab;  // per-row z-pass weight coefficients (FP32 form)
 };
 
