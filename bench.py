@@ -319,7 +319,8 @@ def algorithmic_bytes(family, w, precision, rs, ks):
       zfwd   density in (N * s) + W out (Nc * e)
       yfwd   W in and out (2 Nc e)
       xcorr  W and G in (2 Nc e) + x-pruned Wr out (rs N1 h e)
-             + k-subgrid weight read and read-modify-write (K0 K1 K2 * 24)
+             + k-subgrid weight read (s bytes a cell) and FP64
+             read-modify-write (K0 K1 K2 * (16 + s))
       xcorr00  the ell = 0 term of an autocorrelation: G in (Nc e) + Wr out
              + k-subgrid as xcorr (its transform is a multiple of G)
       yinv   Wr in (rs N1 h e) + Wry out (rs rs h e)
@@ -335,8 +336,8 @@ def algorithmic_bytes(family, w, precision, rs, ks):
     table = {
         "zfwd": n * s + nc * e,
         "yfwd": 2 * nc * e,
-        "xcorr": 2 * nc * e + rs * n1 * h * e + kc * 24,
-        "xcorr00": nc * e + rs * n1 * h * e + kc * 24,
+        "xcorr": 2 * nc * e + rs * n1 * h * e + kc * (16 + s),
+        "xcorr00": nc * e + rs * n1 * h * e + kc * (16 + s),
         "yinv": rs * n1 * h * e + rs * rs * h * e,
         "zinv": rs * rs * h * e + rs ** 3 * 24,
         "weight": n * 8 + n * s,

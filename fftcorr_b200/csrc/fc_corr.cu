@@ -1036,7 +1036,7 @@ size_t correlator_footprint(int kind, const int shape[3], double cell,
     if (precision != FC_FP64)                                // FP32 density,
       bytes += g.ncells() * 4 + (size_t)g.shape[0] * g.shape[1] * 32;  // row table
     const int nlm = maxell == 0 ? 1 : maxell == 2 ? 6 : 15;
-    bytes += (size_t)nlm * g.kcells() * 8;                   // k weights
+    bytes += (size_t)nlm * g.kcells() * rb;                  // k weights
     bytes += (size_t)nlm * g.rsize * g.rsize * g.rsize * 8;  // r weights
   } else {
     bytes += g.nreal_padded() * rb;                          // work

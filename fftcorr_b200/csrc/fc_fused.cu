@@ -253,7 +253,7 @@ template <typename T, int MODE>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     k_xcorr(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
             C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
-            const C2<T> *__restrict__ tabx, const double *__restrict__ ktab) {
+            const C2<T> *__restrict__ tabx, const T *__restrict__ ktab) {
   using C = C2<T>;
   constexpr int B = Tile<T>::B;
   constexpr int BP = B + 1;
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
                                       : ((ox - i) % g.n0 + g.n0) % g.n0;
               const double re = (double)buf[x * BP + b].x;
               const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
-              ksub[cell] += ktab[cell] * re;
+              ksub[cell] += (double)ktab[cell] * re;
             }
           }
         }
@@ -506,7 +506,7 @@ template <typename T, int L, int MODE>
 __global__ void __launch_bounds__(P2<T, L>::THREADS)
     k_xcorr_p2(const C2<T> *__restrict__ W, const C2<T> *__restrict__ G,
                C2<T> *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
-               const C2<T> *__restrict__ tabx, const double *__restrict__ ktab,
+               const C2<T> *__restrict__ tabx, const T *__restrict__ ktab,
                T w00) {
   using C = C2<T>;
   using Q = P2<T, L>;
@@ -584,7 +584,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
                                       : ((ox - i) % L + L) % L;
               const double re = (double)exf(x)->x;
               const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
-              ksub[cell] += ktab[cell] * re;
+              ksub[cell] += (double)ktab[cell] * re;
             }
           }
         }
@@ -938,7 +938,8 @@ __global__ void k_rtable(double *__restrict__ tab, int rs,
 // W(kz)) with make_ylm's arithmetic (correlator.h:453-466), computed once
 // per correlator and multipole so the extraction in the x pass is a
 // multiply-add.
-__global__ void k_ktable(double *__restrict__ tab, int k0, int k1, int k2,
+template <typename KT>
+__global__ void k_ktable(KT *__restrict__ tab, int k0, int k1, int k2,
                          const double *__restrict__ kx,
                          const double *__restrict__ ky,
                          const double *__restrict__ kz,
@@ -952,7 +953,7 @@ __global__ void k_ktable(double *__restrict__ tab, int k0, int k1, int k2,
     const int j = (int)((c / k2) % k1);
     const int i = (int)(c / ((size_t)k2 * k1));
     const double inv_w = 1.0 / (wx[i] * wy[j] * wz[k]);
-    tab[c] = ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
+    tab[c] = (KT)ylm_eval(pk, inv_w, kx[i], ky[j], kz[k]);
   }
 }
 
@@ -1254,8 +1255,9 @@ void FusedSurvey::yfwd(cudaStream_t s) {
 }
 
 template <typename T>
-void FusedSurvey::xcorr(bool product, double *ksub, const double *ktab,
+void FusedSurvey::xcorr(bool product, double *ksub, const void *ktab_v,
                         cudaStream_t s) {
+  const T *ktab = static_cast<const T *>(ktab_v);
   if (is_p2(g.n0)) {
     with_p2(g.n0, [&]<int L>() {
       using Q = P2<T, L>;
@@ -1289,8 +1291,9 @@ void FusedSurvey::xcorr(bool product, double *ksub, const double *ktab,
 }
 
 template <typename T>
-void FusedSurvey::xcorr00(double *ksub, const double *ktab, double w00,
+void FusedSurvey::xcorr00(double *ksub, const void *ktab_v, double w00,
                           cudaStream_t s) {
+  const T *ktab = static_cast<const T *>(ktab_v);
   with_p2(g.n0, [&]<int L>() {
     using Q = P2<T, L>;
     dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
@@ -1358,19 +1361,29 @@ const double *FusedSurvey::r_table(int ell, int m, const double *raxis,
   return b.as<double>();
 }
 
-const double *FusedSurvey::k_table(int ell, int m, const KAxes &ka,
-                                   cudaStream_t s) {
+const void *FusedSurvey::k_table(int ell, int m, const KAxes &ka,
+                                 cudaStream_t s) {
   const int key = ell * 16 + (m + ell);
   auto it = ktabs.find(key);
-  if (it != ktabs.end()) return it->second.as<double>();
+  if (it != ktabs.end()) return it->second.get();
   const size_t n = (size_t)g.ks0 * g.ks1 * g.ks2;
   DeviceBuffer &b = ktabs[key];
-  b.resize(std::max<size_t>(n, 1) * sizeof(double));
-  k_ktable<<<grid_for(n, 256), 256, 0, s>>>(
-      b.as<double>(), g.ks0, g.ks1, g.ks2, ka.kx, ka.ky, ka.kz, ka.wx, ka.wy,
-      ka.wz, make_ylm_params(ell, m, 4.0 * M_PI));
+  const YlmParams pk = make_ylm_params(ell, m, 4.0 * M_PI);
+  // FP64 weights for the FP64 form; the FP32 form keeps them in FP32 (a
+  // relative rounding of 6e-8, far inside its precision).
+  if (fp64_) {
+    b.resize(std::max<size_t>(n, 1) * sizeof(double));
+    k_ktable<double><<<grid_for(n, 256), 256, 0, s>>>(
+        b.as<double>(), g.ks0, g.ks1, g.ks2, ka.kx, ka.ky, ka.kz, ka.wx, ka.wy,
+        ka.wz, pk);
+  } else {
+    b.resize(std::max<size_t>(n, 1) * sizeof(float));
+    k_ktable<float><<<grid_for(n, 256), 256, 0, s>>>(
+        b.as<float>(), g.ks0, g.ks1, g.ks2, ka.kx, ka.ky, ka.kz, ka.wx, ka.wy,
+        ka.wz, pk);
+  }
   FC_LAUNCH_CHECK();
-  return b.as<double>();
+  return b.get();
 }
 
 void FusedSurvey::grid2(const void *rho_in, cudaStream_t s, const KAxes &ka) {
@@ -1394,7 +1407,7 @@ int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
                        PhaseHook *hook, bool g_of_input) {
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
-  const double *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
+  const void *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
   const double *rtab = r_table(ell, m, raxis, pr, s);
   const bool from_g = ell == 0 && g_of_input && is_p2(g.n0);
   auto run = [&](auto tag) {

@@ -78,11 +78,12 @@ class FusedSurvey {
   template <typename T>
   void yfwd(cudaStream_t s);
   template <typename T>
-  void xcorr(bool product, double *ksub, const double *ktab, cudaStream_t s);
+  void xcorr(bool product, double *ksub, const void *ktab, cudaStream_t s);
   template <typename T>
-  void xcorr00(double *ksub, const double *ktab, double w00, cudaStream_t s);
+  void xcorr00(double *ksub, const void *ktab, double w00, cudaStream_t s);
   // Weights of the k-subgrid cells for (ell, m), built on first use.
-  const double *k_table(int ell, int m, const KAxes &ka, cudaStream_t s);
+  // (FP64 for the FP64 form, FP32 for the FP32-mixed form)
+  const void *k_table(int ell, int m, const KAxes &ka, cudaStream_t s);
   // Y_lm(r) of the r-subgrid cells for (ell, m), built on first use.
   const double *r_table(int ell, int m, const double *raxis,
                         const YlmParams &pr, cudaStream_t s);
