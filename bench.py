@@ -299,7 +299,7 @@ def kernel_profile(job, dD, nD, dR, nR):
 TRAFFIC_PER_LAUNCH_512 = {
     "zfwd": 1055.39e6,
     "yfwd": 1064.94e6,
-    "xcorr": 1391.60e6,
+    "xcorr": 1371.43e6,
 }
 
 
