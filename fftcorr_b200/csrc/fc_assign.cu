@@ -275,14 +275,29 @@ __global__ void k_unit_ranges(const uint32_t *__restrict__ units, int64_t nu,
                               const int64_t *__restrict__ coff, int ncolors,
                               unsigned *__restrict__ cnt,
                               uint4 *__restrict__ ranges) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nu;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = units[i];
-    const uint32_t ts = start[u], te = start[u + 1];
-    if (ts >= te) continue;
+  // The loop is warp-uniform so that the lanes of a warp that hold
+  // non-empty units of the same colour take their slots with one atomic.
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < nu;
+       i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    uint32_t u = 0, ts = 0, te = 0;
     int c = 0;
-    while (c + 1 < ncolors && i >= coff[c + 1]) ++c;
-    const unsigned slot = atomicAdd(&cnt[c], 1u);
+    if (i < nu) {
+      u = units[i];
+      ts = start[u];
+      te = start[u + 1];
+      while (c + 1 < ncolors && i >= coff[c + 1]) ++c;
+    }
+    const bool ne = i < nu && ts < te;
+    const unsigned act = __ballot_sync(0xffffffffu, ne);
+    if (!ne) continue;
+    const unsigned grp = __match_any_sync(act, c);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(grp) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(&cnt[c], (unsigned)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const unsigned slot = base + (unsigned)__popc(grp & ((1u << lane) - 1u));
     ranges[coff[c] + slot] = make_uint4(u, ts, te, 0u);
   }
 }
