@@ -17,9 +17,11 @@ result readback inside the timed region); `fp64_gpu` is the plain FP64 GPU
 form on the same inputs.  Inputs are GBs, far larger than the 126 MB L2, so
 no explicit L2 flush is needed between steps.
 
-`--impl reference` times the reference's own C++ (compiled from its sources
-with the project FFT shim, OpenMP, all host threads) on a bounded sample of
-the same job and reports the extrapolated jobs/s.
+`cpu_baseline` and `--impl reference` time the reference's own C++ classes
+(compiled from its sources with the project FFT shim, OpenMP, all host
+threads) on whole jobs of the same workload and the same catalogs; the
+reference's FP64 tables from the baseline job are what `vs_reference_fp64`
+measures both GPU forms against.
 """
 import argparse
 import ctypes
@@ -61,6 +63,7 @@ def parse():
     ap.add_argument("--served-slots", type=int, default=2)
     ap.add_argument("--mix-jobs", type=int, default=48)
     ap.add_argument("--mix-rate", type=float, default=6.0)
+    ap.add_argument("--reference-budget-s", type=float, default=150.0)
     return ap.parse_args()
 
 
@@ -594,102 +597,119 @@ def run_served(a, w, timer):
 
 # --------------------------------------------------------- CPU baseline
 
-def cpu_baseline_sample(w, R, threads):
-    """Times the reference C++ (OpenMP build) on a bounded sample and
-    extrapolates to one job.  Returns (jobs_per_s, description)."""
+REFERENCE_LABEL = ("reference C++ (cc/ MassAssignor + Correlator, -O3 OpenMP "
+                   "-DFFTSLAB, project FFT shim; FFTW unavailable)")
+
+
+def reference_job(w, D, R, threads):
+    """One whole survey job through the reference's own C++ classes on the
+    host cores: MassAssignor (CLI buffer 1e6) on D and on R' into two grids,
+    NN = D + R', Correlator autocorrelation of NN and of RR = R' at the
+    workload's full size.  Timed by the wall clock around the calls.
+    Returns (seconds, nn, rr, phases) or None when oracle/_ref is missing."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    lib_path = os.path.join(ROOT, "oracle", "_ref", "libfcref_omp.so")
-    if not os.path.exists(lib_path):
-        return None, "oracle/_ref/libfcref_omp.so missing"
-    L = ctypes.CDLL(lib_path)
-    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
-    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))  # noqa: E731
-    nsample = min(10_000_000, R.shape[0])
-    sample = np.ascontiguousarray(R[:nsample])
-    shape = np.array(w.ngrid, dtype=np.intc)
-    grid = np.zeros(w.ngrid)
-    st = np.zeros(6)
+    from oracle import ref_lib
+    if not ref_lib.available("omp"):
+        return None
     t0 = time.perf_counter()
-    rc = L.fcref_mass_assign(dp(sample), ctypes.c_long(nsample), ip(shape),
-                             dp(np.asarray(w.posmin, dtype=np.float64)),
-                             ctypes.c_double(w.cell), 1, 0, ctypes.c_long(1000000),
-                             dp(grid), dp(st), 1)
-    t_ma = time.perf_counter() - t0
-    if rc != 0:
-        return None, "reference mass assignment failed"
-    nrows = 1
-    nr = int(math.floor(w.rmax / w.dr))
-    nk = int(math.floor(w.kmax / w.dk))
-    bufs = [np.zeros(nr), np.zeros((nrows, nr), dtype=np.intc), np.zeros((nrows, nr)),
-            np.zeros(nk), np.zeros((nrows, nk), dtype=np.intc), np.zeros((nrows, nk))]
-    zl = ctypes.c_double()
-    timers = np.zeros(8)
-    t0 = time.perf_counter()
-    rc = L.fcref_correlate(
-        1, dp(grid), None, ip(shape), ctypes.c_double(w.cell),
-        dp(np.asarray(w.posmin, dtype=np.float64)), 2, ctypes.c_double(w.rmax),
-        ctypes.c_double(w.dr), ctypes.c_double(w.kmax), ctypes.c_double(w.dk), 0,
-        dp(bufs[0]), ip(bufs[1]), dp(bufs[2]), dp(bufs[3]), ip(bufs[4]), dp(bufs[5]),
-        ctypes.byref(zl), 1, dp(timers))
-    t_corr = time.perf_counter() - t0
-    if rc != 0:
-        return None, "reference correlation failed"
-    setup, _, fft, extract, mult, ylm, hist, total = timers
-    t_fft = fft / 4.0   # ell_max = 0: grid2, the reference's extra grid1, r2c, c2r
-    t_lm = 2 * t_fft + ylm + mult + extract + hist
-    n_lm = sum(2 * l + 1 for l in range(0, w.maxell + 1, 2))
-    corr_job = setup + total + (n_lm - 1) * t_lm
-    # The reference CLI flow assigns D+R' for NN and R' again for RR.
-    ma_job = t_ma * (2 * w.nr + w.nd) / nsample
-    job = ma_job + 2 * corr_job
-    desc = (f"reference C++ (cc/, OpenMP -DFFTSLAB, project FFT shim; FFTW "
-            f"unavailable) on {threads} threads: MassAssignor on {nsample} of the "
-            f"randoms (buffer 1e6) scaled to {2 * w.nr + w.nd} assignments, plus "
-            f"one Correlator run at {w.ngrid[0]}^3 with ell_max=0 timed by the "
-            f"reference's own timers and extrapolated to {n_lm} (ell,m) terms; "
-            f"sample wall {t_ma + t_corr:.1f} s")
-    return 1.0 / job, desc
+    nn, rr, phases = ref_lib.survey_job(D, R, w.ngrid, w.posmin, w.cell, 2, w.rmax,
+                                        w.dr, w.kmax, w.dk, w.maxell, scheme=1,
+                                        build="omp")
+    secs = time.perf_counter() - t0
+    for key, res in (("nn", nn), ("rr", rr)):
+        setup, _, fft, extract, mult, ylm, hist, total = res["timers"]
+        phases[key + "_reference_timers"] = {
+            "setup": setup, "fft": fft, "extract": extract, "multiply": mult,
+            "ylm": ylm, "histogram": hist, "total": total}
+    return secs, nn, rr, phases
+
+
+def reference_sample_desc(w, threads, phases):
+    return (f"{REFERENCE_LABEL} on {threads} threads: one whole job on the full "
+            f"workload ({w.nd} data + {w.nr} randoms assigned, two "
+            f"{w.ngrid[0]}^3 ell<={w.maxell} correlations), wall clock; "
+            f"mass assignment {phases['mass_assign_s']:.1f} s, correlations "
+            f"{phases['correlate_s']:.1f} s")
+
+
+def maxdev_over_rms0(got, ref):
+    """max |got_l - ref_l| / rms(ref_0) for every multipole row l."""
+    got, ref = np.atleast_2d(got), np.atleast_2d(ref)
+    rms0 = float(np.sqrt(np.mean(ref[0] ** 2)))
+    return [float(np.max(np.abs(got[i] - ref[i]))) / rms0 for i in range(ref.shape[0])]
+
+
+def deviations(res, ref):
+    """Per-multipole deviations of one form's (nn, rr, xi) from another's."""
+    (nn, rr, xi), (rnn, rrr, rxi) = res, ref
+    return {"xi": maxdev_over_rms0(xi.T, rxi.T),
+            "NN": maxdev_over_rms0(nn["rhist"], rnn["rhist"]),
+            "RR": maxdev_over_rms0(rr["rhist"], rrr["rhist"]),
+            "P": maxdev_over_rms0(nn["khist"], rnn["khist"]),
+            "counts_equal": bool(np.array_equal(nn["rcounts"], rnn["rcounts"]) and
+                                 np.array_equal(nn["kcounts"], rnn["kcounts"]))}
 
 
 # ------------------------------------------------------------------ main
 
-def run_reference(a, rank):
+def run_reference(a, rank, world):
+    """The reference arm: whole jobs through the reference C++ on all host
+    threads, as many as fit a bounded run (at least one); rank 0 only."""
     if rank != 0:
         return
     w = Workload(a)
     threads = os.cpu_count() or 1
-    from fftcorr_b200 import mocks
-    R = mocks.sector_randoms(min(int(a.nr), 10_000_000), 3, sector=w.sector)
-    R[:, 3] *= -1.0
-    vals = []
-    desc = ""
-    for i in range(a.warmup + a.steps):
-        v, desc = cpu_baseline_sample(w, R, threads)
-        if v is None:
-            print(json.dumps({"impl": "reference", "unavailable": desc}))
-            return
-        if i >= a.warmup:
-            vals.append(v)
-    value = float(np.median(vals))
+    D, R = w.catalogs()
+    from oracle import ref_lib
+    if not ref_lib.available("omp"):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libfcref_omp.so not built"}))
+        return
+    times = []
+    phases = None
+    budget = a.reference_budget_s
+    t_start = time.perf_counter()
+    while len(times) < max(1, a.steps):
+        out = reference_job(w, D, R, threads)
+        times.append(out[0])
+        phases = out[3]
+        if time.perf_counter() - t_start + out[0] > budget:
+            break
+    secs = float(np.mean(times))
+    value = 1.0 / secs
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "jobs/s",
-        "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "n_gpus": 0, "steps": len(times), "warmup": 0,
+        "steps_requested": a.steps, "warmup_requested": a.warmup,
+        "ms_per_step": 1000.0 * secs, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": w.describe(),
+        "data": "synthetic (seeded mock survey catalogs, see config)",
+        "config": bench_config(w, world),
+        "timing": ("every step is one whole job on the full workload, timed by "
+                   "the wall clock; as many steps as fit the arm's bounded run "
+                   f"({budget:.0f} s), no warm-up jobs (CPU code; each job "
+                   "allocates and pages in its own arrays); the host compute_xi "
+                   "(about 1 ms) is not included"),
+        "job_seconds": times,
+        "phases": phases,
         "cpu_baseline": {"value": value, "unit": "jobs/s", "cores": threads,
-                         "kind": "reference", "sample": desc},
+                         "kind": "reference",
+                         "sample": reference_sample_desc(w, threads, phases)},
         "e2e": {"value": value, "unit": "jobs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
+def bench_config(w, world):
+    return dict(w.describe(), parallelism=f"replicas x{world}")
+
+
 def main():
     a = parse()
     rank, world, local = dist_env()
     if a.impl == "reference":
-        run_reference(a, rank)
+        run_reference(a, rank, world)
         return
     from fftcorr_b200 import _lib
     _lib.call("fc_set_device", local)
@@ -742,24 +762,18 @@ def main():
     t_e2e = dist.max(run_e2e_served(a, w, D, R, timer))
 
     fp64 = None
+    res64 = None
     if not a.no_fp64:
         job64 = SurveyJob(w, "fp64")
         t64, (nn64, rr64, xi64) = timed(lambda: job64.run_device(dD, nD, dR, nR),
                                         a.steps, 1)
         prof64 = kernel_profile(job64, dD, nD, dR, nR)
+        res64 = (nn64, rr64, xi64)
         del job64
-        # Largest deviation of every FP32-mixed multipole from the FP64 run,
-        # relative to the rms of its monopole.
-        def maxdev(a32, a64):
-            rms0 = float(np.sqrt(np.mean(a64[:, 0] ** 2)))
-            return [float(np.max(np.abs(a32[:, l] - a64[:, l])) / rms0)
-                    for l in range(a64.shape[1])]
         fp64 = {
             "value": world * a.steps / t64, "unit": "jobs/s",
             "ms_per_step": 1000.0 * t64 / a.steps,
-            "fp32_vs_fp64_xi_maxdev_over_rms_xi0": maxdev(xi, xi64),
-            "fp32_vs_fp64_NN_maxdev_over_rms_0": maxdev(nn["rhist"].T, nn64["rhist"].T),
-            "fp32_vs_fp64_P_maxdev_over_rms_P0": maxdev(nn["khist"].T, nn64["khist"].T),
+            "fp32_vs_fp64_gpu_maxdev_over_rms_0": deviations(res32, res64),
             "kernels": prof64,
         }
 
@@ -793,13 +807,29 @@ def main():
     batched = None if a.no_batched else run_batched(a, None)
     served = None if a.no_served else run_served(a, w, timer)
 
+    # CPU baseline: one whole job through the reference C++ on the same
+    # catalogs; its FP64 tables are also the reference the GPU forms'
+    # deviations are measured against.
     cpu = None
+    vs_reference = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cv, desc = cpu_baseline_sample(w, R, threads)
-        if cv is not None:
-            cpu = {"value": cv, "unit": "jobs/s", "cores": threads,
-                   "kind": "reference", "sample": desc}
+        out = reference_job(w, D, R, threads)
+        if out is not None:
+            secs, rnn, rrr, phases = out
+            cpu = {"value": 1.0 / secs, "unit": "jobs/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": reference_sample_desc(w, threads, phases),
+                   "phases": phases}
+            from fftcorr_b200.correlate import compute_xi
+            ref = (rnn, rrr, compute_xi(rnn["rhist"].T, rrr["rhist"].T))
+            vs_reference = {
+                "what": "max |GPU - reference FP64| / rms(row 0) per multipole "
+                        "(ell = 0, 2, 4) of xi (compute_xi of NN, RR), the NN and "
+                        "RR correlation histograms and P (NN); same catalogs",
+                "fp32_mixed": deviations(res32, ref),
+                "fp64": deviations(res64, ref) if fp64 else None,
+            }
 
     if rank == 0:
         line = {
@@ -808,8 +838,8 @@ def main():
             "ms_per_step": 1000.0 * t_dev / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded mock survey catalogs, see config)",
-            "config": dict(w.describe(), parallelism=f"replicas x{world}",
-                           form="fp32-mixed, inputs resident in HBM"),
+            "config": bench_config(w, world),
+            "form": "fp32-mixed, inputs resident in HBM",
             "e2e": {"value": e2e_value, "unit": "jobs/s",
                     "h2d_bytes_per_step": int(D.nbytes + R.nbytes),
                     "d2h_bytes_per_step": int(result_bytes),
@@ -829,6 +859,7 @@ def main():
                                         "scatter": ma_stats.window_time},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "vs_reference_fp64": vs_reference,
             "gpu_launches": launches_dev,
             "catalog_generation_s": t_gen,
             "batched": batched,

@@ -37,4 +37,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FFTCORR_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_TREE (or set FFTCORR_REFERENCE)")
+    main(ref)
