@@ -201,7 +201,7 @@ __global__ void k_keys(const double *posw, int64_t base, int64_t n,
       ++added;
     }
     keys[pi] = key;
-    vals[pi] = (uint32_t)pi;
+    if (vals) vals[pi] = (uint32_t)pi;
   }
   // Integer counts are exact whatever the order.
   unsigned long long a = added;
@@ -300,6 +300,34 @@ __global__ void k_unit_ranges(const uint32_t *__restrict__ units, int64_t nu,
     const unsigned slot = base + (unsigned)__popc(grp & ((1u << lane) - 1u));
     ranges[coff[c] + slot] = make_uint4(u, ts, te, 0u);
   }
+}
+
+// Exclusive prefix sum over the block (blockDim.x a multiple of 32, at most
+// 1024); sh32 holds 32 words.  Every thread must call it.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v,
+                                                         uint32_t *sh32) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh32[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    uint32_t w = lane < nw ? sh32[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < nw) sh32[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t before = warp ? sh32[warp - 1] : 0u;
+  return before + x - v;
 }
 
 // K-scatter for one colour pass.  Shared memory layout:
@@ -416,12 +444,12 @@ __global__ void __launch_bounds__(kScatterThreads)
 // chunks: all threads gather positions and weights in parallel into shared
 // memory (fractional cell offsets and weight), then each thread walks its
 // own cell's particles of the chunk in sorted order and accumulates the W^3
-// products wx[a]*wy[b]*wz[c] in registers (S_h[a][b][c]).  The footprint
-// sums are then formed in W^3 rounds: in round o every home cell h adds
-// S_h[o] to footprint cell h + o, with a barrier between rounds, so each
-// footprint cell adds its terms in the order o.  Each cell's particles are
-// summed in sorted order whatever the chunking, so the grid is the same
-// bits on every run.
+// products wx[a]*wy[b]*wz[c] in registers (S_h[a][b][c]).  The home cells'
+// sums then go to a shared table S[o][h], and each footprint cell f adds
+// the terms S[o][f - o] of the home cells that reach it in the order o
+// (one barrier, where a scatter into the footprint would need one per o).
+// Each cell's particles are summed in sorted order whatever the chunking,
+// so the grid is the same bits on every run.
 // Scatter unit width along x for the narrow stencils: 2 x 8 x 8 home cells
 // per CTA of 128 threads, five CTAs per SM.
 constexpr int kUnitX = 2;
@@ -436,9 +464,17 @@ struct ScatterP {
   static constexpr int FY = kTile + W - 1;  // ... along y and z
   static constexpr int F3 = FX * FY * FY;
   static constexpr int C = TX * 256;  // particles staged per chunk
-  // pd[C][4] | acc[F3] | gfoot[F3] doubles, pc[C] | cstart[THREADS + 1] ints
-  static constexpr size_t smem =
-      (size_t)C * 36 + (size_t)F3 * 16 + (size_t)(THREADS + 1) * 4;
+  static constexpr int NW = THREADS / 32;
+  static constexpr int ROUNDS = C / THREADS;  // rounds of 32 items per warp
+  // The staged particles pd[C][4] and, once a unit's particles are summed,
+  // the home-cell table S[W3][THREADS] share the first region.
+  static constexpr size_t REGION0 =
+      (size_t)C * 4 > (size_t)W3 * THREADS ? (size_t)C * 4 : (size_t)W3 * THREADS;
+  // region0 | acc[F3] | gfoot[F3] doubles,
+  // perm[C] | wc[NW][THREADS] | cstart[THREADS + 1] ints
+  static constexpr size_t smem = REGION0 * 8 + (size_t)F3 * 16 + (size_t)C * 4 +
+                                 (size_t)NW * THREADS * 4 +
+                                 (size_t)(THREADS + 1) * 4;
 };
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
@@ -455,14 +491,6 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-__device__ __forceinline__ int lower_bound_smem(const int *a, int n, int v) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (a[mid] < v) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
 
 // Global cell of footprint cell (fx, fy, fz) of a unit at (o0, o1, o2) on a
 // grid at least a footprint wide (one wrap at most per axis).
@@ -497,15 +525,22 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
   constexpr int NS = kTile / TX;
   constexpr int OMIN = Stencil<S>::OMIN;
   constexpr int kSlots = C / T;
+  constexpr int NW = Q::NW;
+  constexpr int R = Q::ROUNDS;
   static_assert(C % T == 0, "whole staging slots per thread");
   extern __shared__ __align__(16) double smem[];
   double *pd = smem;                                     // [C][4]
-  double *acc = pd + 4 * C;                              // [F3]
+  double *stab = smem;                                   // [W3][T], after pd
+  double *acc = smem + Q::REGION0;                       // [F3]
   double *gfoot = acc + F3;                              // [F3]
-  int *pc = reinterpret_cast<int *>(gfoot + F3);         // [C]
-  int *cstart = pc + C;                                  // [T + 1]
+  int *perm = reinterpret_cast<int *>(gfoot + F3);       // [C]
+  int *wcs = perm + C;                                   // [NW][T]
+  int *cstart = wcs + NW * T;                            // [T + 1]
   __shared__ uint4 s_rg;
   __shared__ unsigned s_next;
+  __shared__ uint32_t s_scan[32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
 
   const unsigned n = *count;
   if (threadIdx.x == 0) {
@@ -517,7 +552,6 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
   uint4 rg = s_rg;
   unsigned inext = s_next;
   const int h = threadIdx.x;
-  const int hx = h >> 6, hy = (h >> 3) & 7, hz = h & 7;
   const bool direct = g.n[0] >= FX && g.n[1] >= FY && g.n[2] >= FY;
   const bool a16 = (reinterpret_cast<uintptr_t>(posw) & 15) == 0;
   while (rg.y < rg.z) {
@@ -541,9 +575,8 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
     // global cell: copy its current value now, so the latency of the final
     // read-modify-write overlaps the particle gather.  (No other CTA of this
     // colour pass touches these cells.)  The first chunk's wait covers it.
-    for (int f = h; f < F3; f += T) {
-      acc[f] = 0.0;
-      if (direct)
+    if (direct) {
+      for (int f = h; f < F3; f += T)
         cp_async8(gfoot + f, grid + foot_cell<OMIN>(f / (FY * FY), (f / FY) % FY,
                                                     f % FY, o0, o1, o2, g));
     }
@@ -554,20 +587,14 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
     for (uint32_t c0 = ts; c0 < te; c0 += C) {
       const int m = (int)min((uint32_t)C, te - c0);
       if (c0 != ts) __syncthreads();  // the previous chunk has been consumed
-      // Each thread stages up to kSlots particles: all index and key loads
-      // first, then the position gathers as asynchronous copies, so the
-      // gathers of one thread overlap.  Each thread converts its own copies.
+      // Each thread stages up to kSlots particles: the index loads first,
+      // then the catalog rows as asynchronous copies, so the gathers of one
+      // thread overlap.
       uint32_t idx[kSlots];
-      KeyT kk[kSlots];
 #pragma unroll
       for (int j = 0; j < kSlots; ++j) {
         const int i = h + j * T;
-        idx[j] = 0u;
-        kk[j] = kbase;
-        if (i < m) {
-          idx[j] = vals[c0 + i];
-          kk[j] = keys[c0 + i];
-        }
+        idx[j] = i < m ? vals[c0 + i] : 0u;
       }
 #pragma unroll
       for (int j = 0; j < kSlots; ++j) {
@@ -582,9 +609,35 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
 #pragma unroll
           for (int k = 0; k < 4; ++k) cp_async8(d + k, p + k);
         }
-        pc[i] = (int)(kk[j] - kbase);
+      }
+      // Stable order by home cell: warp w ranks its R rounds of 32 items
+      // (items [w*32R, (w+1)*32R)) among equal cells with a running count
+      // per cell in its row of wcs.
+      int *wc = wcs + warp * T;
+      for (int k = lane; k < T; k += 32) wc[k] = 0;
+      __syncwarp();
+      int lcell[R], lrank[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = warp * 32 * R + r * 32 + lane;
+        // (A key outside this unit cannot occur in a correct sort; it is
+        // dropped rather than indexing outside the unit's cells.)
+        const KeyT kd = i < m ? keys[c0 + i] - kbase : (KeyT)T;
+        const int cell = kd < (KeyT)T ? (int)kd : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, cell);
+        const int leader = __ffs(peers) - 1;
+        int b = 0;
+        if (lane == leader && cell >= 0) {
+          b = wc[cell];
+          wc[cell] = b + __popc(peers);
+        }
+        b = __shfl_sync(0xffffffffu, b, leader);
+        lcell[r] = cell;
+        lrank[r] = b + __popc(peers & lt);
+        __syncwarp();
       }
       cp_async_wait_all();
+      // Each thread converts its own rows to (rx, ry, rz, w).
 #pragma unroll
       for (int j = 0; j < kSlots; ++j) {
         const int i = h + j * T;
@@ -596,12 +649,29 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
         d[1] = x[1] - floor(x[1]);
         d[2] = x[2] - floor(x[2]);
       }
-      __syncthreads();  // also orders the zeroing of acc before the first offset
-      cstart[h] = lower_bound_smem(pc, m, h);
-      if (h == 0) cstart[T] = m;
+      __syncthreads();
+      // Cell h: its first position, then each warp's first position in it.
+      int tot = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) tot += wcs[w * T + h];
+      int run = (int)block_exclusive_scan((uint32_t)tot, s_scan);
+      cstart[h] = run;
+      if (h == T - 1) cstart[T] = run + tot;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const int c = wcs[w * T + h];
+        wcs[w * T + h] = run;
+        run += c;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (lcell[r] >= 0)
+          perm[wc[lcell[r]] + lrank[r]] = warp * 32 * R + r * 32 + lane;
       __syncthreads();
       const int lo = cstart[h], hi = cstart[h + 1];
-      for (int i = lo; i < hi; ++i) {
+      for (int q = lo; q < hi; ++q) {
+        const int i = perm[q];
         double wx[W], wy[W], wz[W];
         Stencil<S>::weights(pd[4 * i + 0], pd[4 * i + 1], pd[4 * i + 2],
                             pd[4 * i + 3], wx, wy, wz);
@@ -616,21 +686,30 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
           }
       }
     }
-    // Within a round the targets h + o are distinct.
+    __syncthreads();  // every thread is done with the staged particles
 #pragma unroll
-    for (int o = 0; o < W3; ++o) {
-      const int ox = o / (W * W), oy = (o / W) % W, oz = o % W;
-      acc[((hx + ox) * FY + (hy + oy)) * FY + (hz + oz)] += sacc[o];
-      __syncthreads();
-    }
-    if (direct) {
-      for (int f = h; f < F3; f += T) {
-        const double v = 0.0 + acc[f];
-        if (v != 0.0)
-          grid[foot_cell<OMIN>(f / (FY * FY), (f / FY) % FY, f % FY, o0, o1, o2,
-                               g)] = gfoot[f] + v;
+    for (int o = 0; o < W3; ++o) stab[o * T + h] = sacc[o];
+    __syncthreads();
+    // Footprint cell f = h + o takes S[o][h] for every home cell h in the
+    // unit, in the order o, starting from 0.0.
+    for (int f = h; f < F3; f += T) {
+      const int fx = f / (FY * FY), fy = (f / FY) % FY, fz = f % FY;
+      double v = 0.0;
+#pragma unroll
+      for (int o = 0; o < W3; ++o) {
+        const int qx = fx - o / (W * W), qy = fy - (o / W) % W, qz = fz - o % W;
+        if (qx >= 0 && qx < TX && qy >= 0 && qy < kTile && qz >= 0 && qz < kTile)
+          v += stab[o * T + (qx * kTile + qy) * kTile + qz];
       }
-    } else {
+      if (direct) {
+        if (v != 0.0)
+          grid[foot_cell<OMIN>(fx, fy, fz, o0, o1, o2, g)] = gfoot[f] + v;
+      } else {
+        acc[f] = v;
+      }
+    }
+    if (!direct) {
+      __syncthreads();
       // Each global cell is written by one footprint cell (its smallest
       // alias when the footprint wraps onto itself on narrow grids).
       for (int f = h; f < F3; f += T) {
@@ -754,6 +833,9 @@ struct Assignor {
   int64_t count = 0;
   int64_t capacity = 0;
   DeviceBuffer posw, keys, keys_alt, vals, vals_alt, cub_temp;
+  // NGP/CIC/TSC sort by unit only (key bits from unit_shift up): the
+  // scatter orders each unit's particles by cell itself.
+  int unit_shift = 0;
   DeviceBuffer unit_start;             // first sorted particle per unit
   DeviceBuffer color_units;            // units in colour order
   DeviceBuffer unit_ranges;            // uint4 per unit, colour slices
@@ -813,6 +895,7 @@ struct Assignor {
     FC_CUDA(cudaMemsetAsync(totals.get(), 0, totals.bytes(), grid->stream));
     FC_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), grid->stream));
     if (scheme != 2) {
+      while ((1 << unit_shift) < unit_x * kTile * kTile) ++unit_shift;
       if (wide_keys)
         scatter_p_kernel<uint64_t>(scheme, &scatter_fn, &scatter_smem_bytes);
       else
@@ -1036,26 +1119,35 @@ struct Assignor {
     if (buffer_size == 0 || count >= buffer_size) flush();
   }
 
+  // K-sort: stable radix sort of (key, particle index) on key bits
+  // [begin_bit, end_bit).  Returns the sorted arrays.
   template <typename KeyT>
-  void flush_typed() {
+  void sort_keys(int begin_bit, const KeyT **sk, const uint32_t **sv) {
     const int64_t n = count;
-    // K-sort.
     cub::DoubleBuffer<KeyT> dk(keys.as<KeyT>(), keys_alt.as<KeyT>());
     cub::DoubleBuffer<uint32_t> dv(vals.as<uint32_t>(), vals_alt.as<uint32_t>());
     size_t temp = 0;
-    FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, n, 0,
+    FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, n, begin_bit,
                                             end_bit, stream()));
     if (graph_mode)
       FC_REQUIRE(temp <= cub_temp.bytes(), FC_ERR_STATE,
                  "sort scratch was not prepared for this many particles");
     cub_temp.resize(temp);
     if (!graph_mode) sort_timer.start(stream());
-    FC_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp.get(), temp, dk, dv, n, 0,
-                                            end_bit, stream()));
+    FC_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp.get(), temp, dk, dv, n,
+                                            begin_bit, end_bit, stream()));
     if (!graph_mode) sort_timer.stop(stream());
-    const KeyT *sk = dk.Current();
-    const uint32_t *sv = dv.Current();
-    // K-units + K-scatter.
+    *sk = dk.Current();
+    *sv = dv.Current();
+  }
+
+  // D12: sort by cell key, then the tile scatter.
+  template <typename KeyT>
+  void flush_d12() {
+    const int64_t n = count;
+    const KeyT *sk;
+    const uint32_t *sv;
+    sort_keys<KeyT>(0, &sk, &sv);
     if (!graph_mode) window_timer.start(stream());
     const int unit_cells = unit_x * kTile * kTile;
     k_unit_starts<KeyT><<<grid_for(nunits + 1, 256), 256, 0, stream()>>>(
@@ -1063,39 +1155,64 @@ struct Assignor {
     FC_LAUNCH_CHECK();
     const uint32_t *units = color_units.as<uint32_t>();
     const int ncolors = (int)color_offsets.size() - 1;
-    unsigned *counters = pass_counters.as<unsigned>();
-    if (scheme != 2) {
-      FC_CUDA(cudaMemsetAsync(counters, 0, pass_counters.bytes(), stream()));
-      k_unit_ranges<<<grid_for(nunits, 256), 256, 0, stream()>>>(
-          units, nunits, unit_start.as<uint32_t>(), color_off_dev.as<int64_t>(),
-          ncolors, counters, unit_ranges.as<uint4>());
-      FC_LAUNCH_CHECK();
-    }
-    double *gp = grid->ptr();
-    AssignGeom ga = geom;
     for (int c = 0; c < ncolors; ++c) {
       const int64_t nu = color_offsets[c + 1] - color_offsets[c];
       if (nu == 0) continue;
-      if (scheme == 2) {
-        k_scatter<2, KeyT><<<(unsigned)nu, kScatterThreads, scatter_smem<2>(),
-                             stream()>>>(src_posw, sk, sv,
-                                         unit_start.as<uint32_t>(),
-                                         units + color_offsets[c], geom, gp);
-        FC_LAUNCH_CHECK();
-        continue;
-      }
+      k_scatter<2, KeyT><<<(unsigned)nu, kScatterThreads, scatter_smem<2>(),
+                           stream()>>>(src_posw, sk, sv, unit_start.as<uint32_t>(),
+                                       units + color_offsets[c], geom, grid->ptr());
+      FC_LAUNCH_CHECK();
+    }
+    if (!graph_mode) window_timer.stop(stream());
+  }
+
+  // NGP / CIC / TSC: sort by unit, then the persistent unit scatter in
+  // colour passes.
+  template <typename KeyT>
+  void flush_units() {
+    const int64_t n = count;
+    const KeyT *sk;
+    const uint32_t *sv;
+    sort_keys<KeyT>(unit_shift, &sk, &sv);
+    cudaStream_t st = stream();
+    if (!graph_mode) window_timer.start(st);
+    const int unit_cells = unit_x * kTile * kTile;
+    k_unit_starts<KeyT><<<grid_for(nunits + 1, 256), 256, 0, st>>>(
+        sk, n, nunits, unit_cells, unit_start.as<uint32_t>());
+    FC_LAUNCH_CHECK();
+    const uint32_t *units = color_units.as<uint32_t>();
+    const int ncolors = (int)color_offsets.size() - 1;
+    unsigned *counters = pass_counters.as<unsigned>();
+    FC_CUDA(cudaMemsetAsync(counters, 0, pass_counters.bytes(), st));
+    k_unit_ranges<<<grid_for(nunits, 256), 256, 0, st>>>(
+        units, nunits, unit_start.as<uint32_t>(), color_off_dev.as<int64_t>(),
+        ncolors, counters, unit_ranges.as<uint4>());
+    FC_LAUNCH_CHECK();
+    double *gp = grid->ptr();
+    AssignGeom ga = geom;
+    const double *pw = src_posw;
+    for (int c = 0; c < ncolors; ++c) {
+      const int64_t nu = color_offsets[c + 1] - color_offsets[c];
+      if (nu == 0) continue;
       const uint4 *cr = unit_ranges.as<uint4>() + color_offsets[c];
       const unsigned *cnt = counters + c;
       unsigned *nxt = counters + ncolors + c;
-      const double *pw = src_posw;
       void *args[] = {(void *)&pw, (void *)&sk, (void *)&sv, (void *)&cr,
                       (void *)&cnt, (void *)&nxt, (void *)&ga, (void *)&gp};
       const unsigned ctas = (unsigned)std::min<int64_t>(nu, scatter_ctas);
       FC_CUDA(cudaLaunchKernel(scatter_fn, dim3(ctas), dim3(scatter_threads),
-                               args, scatter_smem_bytes, stream()));
+                               args, scatter_smem_bytes, st));
       FC_LAUNCH_CHECK();
     }
-    if (!graph_mode) window_timer.stop(stream());
+    if (!graph_mode) window_timer.stop(st);
+  }
+
+  template <typename KeyT>
+  void flush_typed() {
+    if (scheme == 2)
+      flush_d12<KeyT>();
+    else
+      flush_units<KeyT>();
   }
 
   // MassAssignor::flush (mass_assignor.h:127-191).
