@@ -22,6 +22,8 @@ FC_ERR_STATE = -6
 FC_ERR_UNSUPPORTED = -7
 FC_ERR_TIMEOUT = -8
 FC_ERR_ADMISSION = -9
+FC_FAULT_DEVICE_ALLOC = 1
+FC_FAULT_FFT_PLAN = 2
 
 FC_FP64 = 0
 FC_FP32_MIXED = 1
@@ -196,6 +198,9 @@ _SIGNATURES = {
     "fc_host_unregister": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_device_malloc": (ctypes.c_int, [ctypes.c_size_t, c_void_pp]),
     "fc_device_free": (ctypes.c_int, [ctypes.c_void_p]),
+    "fc_fault_inject": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64]),
+    "fc_set_device_budget": (ctypes.c_int, [ctypes.c_size_t]),
+    "fc_device_bytes": (ctypes.c_int, [ctypes.POINTER(ctypes.c_size_t)]),
     "fc_memcpy_htod": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "fc_memcpy_dtoh": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     "fc_device_memory": (ctypes.c_int, [ctypes.POINTER(ctypes.c_size_t),

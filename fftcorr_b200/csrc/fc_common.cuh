@@ -83,6 +83,21 @@ int guard(F &&f) {
   }
 }
 
+// ------------------------------------------------------- fault injection
+
+// Test hooks behind fc_fault_inject and fc_set_device_budget.  A planned
+// failure is raised on the host where the real one would surface, before
+// the CUDA or cuFFT call is made, so nothing ever faults on the GPU.
+enum FaultKind { kFaultDeviceAlloc = 1, kFaultFftPlan = 2 };
+// True when an armed fault of this kind fires now (it then disarms).
+bool fault_fires(int kind);
+// Called before every device allocation of the library: throws
+// FC_ERR_ALLOC for an injected failure or when the bytes would exceed the
+// budget.
+void device_alloc_check(size_t bytes);
+// Running total of the library's device bytes (for the budget).
+void device_bytes_add(long long delta);
+
 // ---------------------------------------------------------------- buffers
 
 // Owning device allocation (cudaMalloc / cudaFree).
@@ -112,11 +127,16 @@ class DeviceBuffer {
     if (bytes <= bytes_) return;
     release();
     if (bytes == 0) return;
+    device_alloc_check(bytes);
     FC_CUDA(cudaMalloc(&ptr_, bytes));
     bytes_ = bytes;
+    device_bytes_add((long long)bytes);
   }
   void release() {
-    if (ptr_) cudaFree(ptr_);
+    if (ptr_) {
+      cudaFree(ptr_);
+      device_bytes_add(-(long long)bytes_);
+    }
     ptr_ = nullptr;
     bytes_ = 0;
   }

@@ -153,6 +153,34 @@ void device_sum_sumsq(const double *a, size_t n, double *scratch,
   FC_LAUNCH_CHECK();
 }
 
+// ------------------------------------------------------- fault injection
+
+namespace {
+std::atomic<long long> g_fault_countdown[3];  // by FaultKind; <= 0: disarmed
+std::atomic<long long> g_device_bytes{0};
+std::atomic<unsigned long long> g_device_budget{0};  // 0: no budget
+}  // namespace
+
+bool fault_fires(int kind) {
+  std::atomic<long long> &c = g_fault_countdown[kind];
+  long long v = c.load();
+  while (v > 0) {
+    if (c.compare_exchange_weak(v, v - 1)) return v == 1;
+  }
+  return false;
+}
+
+void device_alloc_check(size_t bytes) {
+  if (fault_fires(kFaultDeviceAlloc))
+    FC_THROW(FC_ERR_ALLOC, "injected device allocation failure");
+  const unsigned long long budget = g_device_budget.load();
+  if (budget && (unsigned long long)g_device_bytes.load() + bytes > budget)
+    FC_THROW(FC_ERR_ALLOC, "device memory budget exceeded (" +
+                               std::to_string(bytes) + " more bytes)");
+}
+
+void device_bytes_add(long long delta) { g_device_bytes += delta; }
+
 // ------------------------------------------------------------- the grid
 
 Grid::Grid(const int shp[3], const double pmin[3], double cell) {
@@ -165,9 +193,15 @@ Grid::Grid(const int shp[3], const double pmin[3], double cell) {
   cell_size = cell;
   FC_CUDA(cudaGetDevice(&device));
   FC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  data.resize(size() * sizeof(double));
-  scratch.resize((2 * kSumBlocks + 2) * sizeof(double));
-  clear();
+  try {
+    data.resize(size() * sizeof(double));
+    scratch.resize((2 * kSumBlocks + 2) * sizeof(double));
+    clear();
+  } catch (...) {
+    cudaStreamDestroy(stream);
+    stream = nullptr;
+    throw;
+  }
 }
 
 Grid::~Grid() {
@@ -356,22 +390,14 @@ __global__ void k_seg_partials(const double *a, int64_t n, double *partials) {
   }
 }
 
-std::mutex g_static_mu;
-double *g_static_addr[64] = {nullptr};
-
-// Device address of g_static_scratch on the current device, looked up once
-// per device with that device current.
+// Device address of g_static_scratch in the current device's context, looked
+// up on every call (a cheap query): a cached address would go stale if the
+// context were torn down and created again (cudaDeviceReset), which reloads
+// the module.
 double *static_scratch() {
-  int dev = 0;
-  FC_CUDA(cudaGetDevice(&dev));
-  FC_REQUIRE(dev >= 0 && dev < 64, FC_ERR_UNSUPPORTED, "device index >= 64");
-  std::lock_guard<std::mutex> lock(g_static_mu);
-  if (!g_static_addr[dev]) {
-    void *p = nullptr;
-    FC_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
-    g_static_addr[dev] = static_cast<double *>(p);
-  }
-  return g_static_addr[dev];
+  void *p = nullptr;
+  FC_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+  return static_cast<double *>(p);
 }
 
 }  // namespace
@@ -436,6 +462,26 @@ int fc_device_malloc(size_t bytes, void **ptr) {
     FC_REQUIRE(ptr, FC_ERR_INVALID, "null pointer");
     *ptr = nullptr;
     FC_CUDA(cudaMalloc(ptr, bytes));
+  });
+}
+
+int fc_fault_inject(int kind, int64_t n) {
+  return guard([&] {
+    FC_REQUIRE(kind == FC_FAULT_DEVICE_ALLOC || kind == FC_FAULT_FFT_PLAN,
+               FC_ERR_INVALID, "unknown fault kind");
+    g_fault_countdown[kind].store(n > 0 ? (long long)n : 0);
+  });
+}
+
+int fc_set_device_budget(size_t bytes) {
+  return guard([&] { g_device_budget.store(bytes); });
+}
+
+int fc_device_bytes(size_t *bytes) {
+  return guard([&] {
+    FC_REQUIRE(bytes, FC_ERR_INVALID, "null argument");
+    const long long b = g_device_bytes.load();
+    *bytes = b > 0 ? (size_t)b : 0;
   });
 }
 

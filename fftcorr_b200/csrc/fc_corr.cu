@@ -443,27 +443,45 @@ struct Correlator {
       }
     }
     FC_CUDA(cudaGetDevice(&device));
-    FC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
-    stream = own_stream;
-    FC_CUDA(cudaEventCreate(&ev_start));
-    FC_CUDA(cudaEventCreate(&ev_stop));
-    const char *mode = std::getenv("FFTCORR_B200_FFT");
-    const bool want_fused = !(mode && std::string(mode) == "cufft");
-    if (kind == FC_SURVEY && want_fused &&
-        FusedSurvey::supported(geo.shape, geo.rsize))
-      fused.reset(new FusedSurvey(geo.shape, geo.rsize, geo.kshape, fp64()));
-    allocate();
-    if (!fused) make_plans();
-    build_bins();
+    try {
+      FC_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+      stream = own_stream;
+      FC_CUDA(cudaEventCreate(&ev_start));
+      FC_CUDA(cudaEventCreate(&ev_stop));
+      const char *mode = std::getenv("FFTCORR_B200_FFT");
+      const bool want_fused = !(mode && std::string(mode) == "cufft");
+      if (kind == FC_SURVEY && want_fused &&
+          FusedSurvey::supported(geo.shape, geo.rsize))
+        fused.reset(new FusedSurvey(geo.shape, geo.rsize, geo.kshape, fp64()));
+      allocate();
+      if (!fused) make_plans();
+      build_bins();
+      // Every (ell, m) weight table now: a correlation (a served job on a
+      // resident correlator in particular) then allocates nothing.
+      if (fused)
+        fused->prepare_tables(2 * (geo.nrows - 1), (double)geo.ncells(),
+                              d_raxis.as<double>(), kaxes(),
+                              ksub.as<double>() != nullptr, stream);
+    } catch (...) {
+      // A failed construction leaves no stream, event or plan behind (the
+      // buffers free themselves).
+      release_handles();
+      throw;
+    }
   }
 
-  ~Correlator() {
+  ~Correlator() { release_handles(); }
+
+  void release_handles() {
     if (stream) cudaStreamSynchronize(stream);
     if (plan_r2c) cufftDestroy(plan_r2c);
     if (plan_c2r) cufftDestroy(plan_c2r);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
     if (own_stream) cudaStreamDestroy(own_stream);
+    plan_r2c = plan_c2r = 0;
+    ev_start = ev_stop = nullptr;
+    own_stream = stream = nullptr;
   }
 
   bool fp64() const { return precision == FC_FP64; }
@@ -498,7 +516,20 @@ struct Correlator {
     FC_CUDA(cudaMemset(d_zerolag.get(), 0, d_zerolag.bytes()));
   }
 
+  // Creates both plans; on a failure neither is left behind (the
+  // constructor that calls this does not run the destructor when it throws).
   void make_plans() {
+    try {
+      make_plans_unguarded();
+    } catch (...) {
+      if (plan_r2c) cufftDestroy(plan_r2c);
+      if (plan_c2r) cufftDestroy(plan_c2r);
+      plan_r2c = plan_c2r = 0;
+      throw;
+    }
+  }
+
+  void make_plans_unguarded() {
     // In-place padded r2c / c2r, FftGrid::plan_fft (fft_grid.cc:69-84).
     int n[3] = {geo.shape[0], geo.shape[1], geo.shape[2]};
     int rembed[3] = {geo.shape[0], geo.shape[1], geo.n2p()};
@@ -510,6 +541,8 @@ struct Correlator {
     FC_CUFFT(cufftSetAutoAllocation(plan_r2c, 0));
     FC_CUFFT(cufftSetAutoAllocation(plan_c2r, 0));
     size_t ws1 = 0, ws2 = 0;
+    if (fault_fires(kFaultFftPlan))
+      FC_THROW(FC_ERR_CUFFT, "injected cuFFT plan creation failure");
     FC_CUFFT(cufftMakePlanMany(plan_r2c, 3, n, rembed, 1, (int)std::min<long long>(rdist, 1LL << 30),
                                cembed, 1, (int)std::min<long long>(cdist, 1LL << 30),
                                fp64() ? CUFFT_D2Z : CUFFT_R2C, 1, &ws1));
@@ -1037,7 +1070,7 @@ size_t correlator_footprint(int kind, const int shape[3], double cell,
       bytes += g.ncells() * 4 + (size_t)g.shape[0] * g.shape[1] * 32;  // row table
     const int nlm = maxell == 0 ? 1 : maxell == 2 ? 6 : 15;
     bytes += (size_t)nlm * g.kcells() * rb;                  // k weights
-    bytes += (size_t)nlm * g.rsize * g.rsize * g.rsize * 8;  // r weights
+    bytes += (size_t)nlm * g.rsize * g.rsize * g.rsize * rb; // r weights
   } else {
     bytes += g.nreal_padded() * rb;                          // work
     if (kind == FC_SURVEY) bytes += g.ncomplex() * eb;       // grid2 FFT

@@ -359,7 +359,7 @@ template <typename T>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     k_zinv_rsub(const C2<T> *__restrict__ Wry, double *__restrict__ rsub,
                 FusedGeom g, const C2<T> *__restrict__ tabz,
-                const double *__restrict__ rtab) {
+                const T *__restrict__ rtab) {
   using C = C2<T>;
   constexpr int B = Tile<T>::B;
   constexpr int BP = B + 1;
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     const C zz = buf[(z >> 1) * BP + b];
     const double v = (double)((z & 1) ? zz.y : zz.x);
     const size_t cell = (size_t)row * g.rs + rk;
-    rsub[cell] += rtab[cell] * v;
+    rsub[cell] += (double)rtab[cell] * v;
   }
 }
 
@@ -682,7 +682,7 @@ template <typename T, int L>
 __global__ void __launch_bounds__(P2<T, L>::THREADS)
     k_zinv_p2(const C2<T> *__restrict__ Wry, double *__restrict__ rsub,
               FusedGeom g, const C2<T> *__restrict__ tabz,
-              const double *__restrict__ rtab) {
+              const T *__restrict__ rtab) {
   using C = C2<T>;
   using Q = P2<T, L>;
   constexpr int RP = L + L / 8 + 1;
@@ -727,7 +727,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
       const double val = (double)(h ? v[u].y : v[u].x);
       for (int rk = (z + g.ro) % g.n2; rk < g.rs; rk += g.n2) {
         const size_t cell = (size_t)row * g.rs + rk;
-        rsub[cell] += rtab[cell] * val;
+        rsub[cell] += (double)rtab[cell] * val;
       }
     }
   }
@@ -922,7 +922,8 @@ __global__ void k_rowpoly(float4 *__restrict__ tab, int64_t nrows, int n1,
 // Per-cell r-subgrid weight of one (ell, m): Y_lm(r) with the r-subgrid
 // normalisation (make_ylm, correlator.h:477-480), computed once per
 // correlator and multipole so the z inverse pass does a multiply-add.
-__global__ void k_rtable(double *__restrict__ tab, int rs,
+template <typename RT>
+__global__ void k_rtable(RT *__restrict__ tab, int rs,
                          const double *__restrict__ raxis, YlmParams pr) {
   const size_t n = (size_t)rs * rs * rs;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -930,7 +931,7 @@ __global__ void k_rtable(double *__restrict__ tab, int rs,
     const int rk = (int)(i % rs);
     const int rj = (int)((i / rs) % rs);
     const int ri = (int)(i / ((size_t)rs * rs));
-    tab[i] = ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
+    tab[i] = (RT)ylm_eval(pr, 1.0, raxis[ri], raxis[rj], raxis[rk]);
   }
 }
 
@@ -1328,7 +1329,8 @@ void FusedSurvey::yinv(cudaStream_t s) {
 }
 
 template <typename T>
-void FusedSurvey::zinv(double *rsub, const double *rtab, cudaStream_t s) {
+void FusedSurvey::zinv(double *rsub, const void *rtab_v, cudaStream_t s) {
+  const T *rtab = static_cast<const T *>(rtab_v);
   if (is_p2(g.m)) {
     with_p2(g.m, [&]<int L>() {
       using Q = P2<T, L>;
@@ -1348,17 +1350,33 @@ void FusedSurvey::zinv(double *rsub, const double *rtab, cudaStream_t s) {
   FC_LAUNCH_CHECK();
 }
 
-const double *FusedSurvey::r_table(int ell, int m, const double *raxis,
-                                   const YlmParams &pr, cudaStream_t s) {
+const void *FusedSurvey::r_table(int ell, int m, const double *raxis,
+                                 const YlmParams &pr, cudaStream_t s) {
   const int key = ell * 16 + (m + ell);
   auto it = rtabs.find(key);
-  if (it != rtabs.end()) return it->second.as<double>();
+  if (it != rtabs.end()) return it->second.get();
   const size_t n = (size_t)g.rs * g.rs * g.rs;
   DeviceBuffer &b = rtabs[key];
-  b.resize(std::max<size_t>(n, 1) * sizeof(double));
-  k_rtable<<<grid_for(n, 256), 256, 0, s>>>(b.as<double>(), g.rs, raxis, pr);
+  // FP64 for the FP64 form, FP32 for the FP32-mixed form (the product with
+  // the transform and the accumulation stay FP64).
+  if (fp64_) {
+    b.resize(std::max<size_t>(n, 1) * sizeof(double));
+    k_rtable<double><<<grid_for(n, 256), 256, 0, s>>>(b.as<double>(), g.rs, raxis, pr);
+  } else {
+    b.resize(std::max<size_t>(n, 1) * sizeof(float));
+    k_rtable<float><<<grid_for(n, 256), 256, 0, s>>>(b.as<float>(), g.rs, raxis, pr);
+  }
   FC_LAUNCH_CHECK();
-  return b.as<double>();
+  return b.get();
+}
+
+void FusedSurvey::prepare_tables(int maxell, double ncells, const double *raxis,
+                                 const KAxes &ka, bool with_k, cudaStream_t s) {
+  for (int ell = 0; ell <= maxell; ell += 2)
+    for (int m = -ell; m <= ell; ++m) {
+      r_table(ell, m, raxis, make_ylm_params(ell, m, 4.0 * M_PI / ncells), s);
+      if (with_k) k_table(ell, m, ka, s);
+    }
 }
 
 const void *FusedSurvey::k_table(int ell, int m, const KAxes &ka,
@@ -1408,7 +1426,7 @@ int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
   const void *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
-  const double *rtab = r_table(ell, m, raxis, pr, s);
+  const void *rtab = r_table(ell, m, raxis, pr, s);
   const bool from_g = ell == 0 && g_of_input && is_p2(g.n0);
   auto run = [&](auto tag) {
     using T = decltype(tag);

@@ -52,6 +52,10 @@ class FusedSurvey {
   }
   // G = 3-D DFT of the prepared grid (BaseCorrelator::set_grid2).
   void grid2(const void *rho_in, cudaStream_t s, const KAxes &ka);
+  // Builds the r- (and, with with_k, k-) subgrid weight tables of every
+  // (ell, m) up to maxell, so that later correlations allocate nothing.
+  void prepare_tables(int maxell, double ncells, const double *raxis,
+                      const KAxes &ka, bool with_k, cudaStream_t s);
   // One (ell, m) term of Correlator::correlate_internal, accumulated into
   // the FP64 subgrids.
   // Returns the number of full-grid transforms run (1 or 2).
@@ -84,13 +88,14 @@ class FusedSurvey {
   // Weights of the k-subgrid cells for (ell, m), built on first use.
   // (FP64 for the FP64 form, FP32 for the FP32-mixed form)
   const void *k_table(int ell, int m, const KAxes &ka, cudaStream_t s);
-  // Y_lm(r) of the r-subgrid cells for (ell, m), built on first use.
-  const double *r_table(int ell, int m, const double *raxis,
-                        const YlmParams &pr, cudaStream_t s);
+  // Y_lm(r) of the r-subgrid cells for (ell, m), built on first use, in
+  // the same type as the k weights.
+  const void *r_table(int ell, int m, const double *raxis,
+                      const YlmParams &pr, cudaStream_t s);
   template <typename T>
   void yinv(cudaStream_t s);
   template <typename T>
-  void zinv(double *rsub, const double *rtab, cudaStream_t s);
+  void zinv(double *rsub, const void *rtab, cudaStream_t s);
 
   bool fp64_;
   DeviceBuffer tabx, taby, tabz;

@@ -567,6 +567,7 @@ int fc_server_wait(fc_server *server, uint64_t ticket, double timeout_s,
     else
       s->cv_done.wait_for(g, std::chrono::duration<double>(timeout_s), pred);
     if (done) *done = j->state == 2;
+    FC_REQUIRE(j->state == 2, FC_ERR_TIMEOUT, "the job had not finished");
   });
 }
 

@@ -121,9 +121,15 @@ class Server:
         return t.value
 
     def wait(self, ticket, timeout=None):
+        """True when the job has finished; False when `timeout` seconds ran
+        out first."""
         done = ctypes.c_int()
-        _lib.call("fc_server_wait", self._handle, int(ticket),
-                  -1.0 if timeout is None else float(timeout), ctypes.byref(done))
+        rc = _lib.load().fc_server_wait(self._handle, int(ticket),
+                                        -1.0 if timeout is None else float(timeout),
+                                        ctypes.byref(done))
+        if rc == _lib.FC_ERR_TIMEOUT:
+            return False
+        _lib.check(rc)
         return bool(done.value)
 
     def info(self, ticket):

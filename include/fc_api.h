@@ -342,7 +342,8 @@ int fc_server_create(size_t hbm_budget, int slots, int max_bypass,
 int fc_server_destroy(fc_server *server);
 /* Queues a job; FC_ERR_ADMISSION if it alone exceeds the budget. */
 int fc_server_submit(fc_server *server, const fc_job *job, uint64_t *ticket);
-/* Waits up to timeout_s (< 0: forever); *done = 1 when it finished. */
+/* Waits up to timeout_s (< 0: forever); *done = 1 when it finished.  A
+ * wait that runs out sets *done = 0 and returns FC_ERR_TIMEOUT. */
 int fc_server_wait(fc_server *server, uint64_t ticket, double timeout_s,
                    int *done);
 int fc_server_job_info(fc_server *server, uint64_t ticket, fc_job_info *info);
@@ -445,8 +446,12 @@ int fc_hist_get(const fc_hist *h, double *bins, int *counts, double *hist);
  * point allocates nothing: its scratch is a fixed 64 KiB array in the
  * library's own device memory, which every GPU that loads the library holds
  * until the process exits.  n may be at most FC_SUM_STATIC_MAX_N; larger n
- * is rejected with FC_ERR_RANGE.  The first call on a device looks up the
- * scratch address, so make that first call before any stream capture.  All
+ * is rejected with FC_ERR_RANGE.  Every call looks up the scratch address
+ * in the current context (a query, no allocation), so make calls outside
+ * any stream capture.  The work runs on the legacy default stream: it waits
+ * for work the caller queued on blocking streams of the device (so data
+ * written there is complete), non-blocking streams are not waited for, and
+ * a global-mode stream capture in another thread makes the call fail.  All
  * calls share the one scratch array, so calls that overlap on the GPU (from
  * several host threads) race; this call waits for its result before
  * returning.  Has no counterpart in the reference. */
@@ -466,6 +471,22 @@ int fc_device_synchronize(void);
  * speed (cudaHostRegister), and releases it. */
 int fc_host_register(void *ptr, size_t bytes);
 int fc_host_unregister(void *ptr);
+/* ------------------------------------------------- failure injection */
+/* Test hooks.  A planned failure is raised on the host where the real one
+ * would surface, before the CUDA or cuFFT call, so no GPU faults.  With
+ * FC_FAULT_DEVICE_ALLOC, the n-th device allocation of the library from now
+ * fails with FC_ERR_ALLOC.  With FC_FAULT_FFT_PLAN, the n-th cuFFT plan
+ * creation fails with FC_ERR_CUFFT.  n <= 0 disarms.  The reference fails
+ * the same way on an allocation or an FFTW plan that cannot be made
+ * (cc/grid/fft_grid.cc:126,153). */
+enum { FC_FAULT_DEVICE_ALLOC = 1, FC_FAULT_FFT_PLAN = 2 };
+int fc_fault_inject(int kind, int64_t n);
+/* Caps the device bytes the library's own allocations may hold (0: no cap).
+ * An allocation past the cap fails with FC_ERR_ALLOC. */
+int fc_set_device_budget(size_t bytes);
+/* Device bytes the library's allocations hold now. */
+int fc_device_bytes(size_t *bytes);
+
 /* Plain device allocations for callers that stage inputs themselves. */
 int fc_device_malloc(size_t bytes, void **ptr);
 int fc_device_free(void *ptr);

@@ -51,6 +51,30 @@ def test_static_sum_matches_allocating_sum_on_two_calls():
         _lib.load().fc_grid_destroy(h)
 
 
+@pytest.mark.parametrize("n", [0, (1 << 18) - 1, (1 << 18) + 1])
+def test_static_sum_edge_sizes(n):
+    """No values (the result slots are cleared, not summed), and one value
+    short of and past the size one block sums, whose last block then ends
+    part way."""
+    rng = np.random.default_rng(n + 1)
+    values = rng.normal(size=(1, 1, max(n, 1))) - 0.5
+    h, ptr = _device_grid(values)
+    try:
+        # A call on other data first, so a stale result would show.
+        s, q = ctypes.c_double(), ctypes.c_double()
+        _lib.call("fc_sum_sumsq_static", ptr, values.size, ctypes.byref(s),
+                  ctypes.byref(q))
+        _lib.call("fc_sum_sumsq_static", ptr, n, ctypes.byref(s), ctypes.byref(q))
+        v = values.reshape(-1)[:n]
+        if n == 0:
+            assert s.value == 0.0 and q.value == 0.0
+        else:
+            assert s.value == pytest.approx(float(np.sum(v)), rel=RTOL)
+            assert q.value == pytest.approx(float(np.sum(v * v)), rel=RTOL)
+    finally:
+        _lib.load().fc_grid_destroy(h)
+
+
 def test_static_sum_rejects_sizes_beyond_its_scratch():
     values = np.ones((4, 4, 4))
     h, ptr = _device_grid(values)
