@@ -764,67 +764,96 @@ struct PP {
   }
 };
 
+// The FP32 y passes pair ADJACENT columns: thread (t, p) holds columns 2p
+// and 2p + 1 of the CTA's B and moves both with one 16-byte access, and B
+// is 16 where the CTA allows it, so a warp's access covers whole 128-byte
+// row segments.  (Row pitches are multiples of 16 columns, so the pair of
+// the last valid column lies in the padding and is read but never stored.)
 template <int L>
-__global__ void __launch_bounds__(PP<L>::THREADS)
-    k_yfwd_pp(float2 *__restrict__ W, FusedGeom g,
-              const float2 *__restrict__ taby) {
-  using Q = PP<L>;
-  extern __shared__ unsigned char smem_raw[];
-  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
-  const int t = threadIdx.x / Q::PB;
-  const int p = threadIdx.x - t * Q::PB;
-  const int c0 = blockIdx.x * Q::B + p, c1 = c0 + Q::PB;
-  const bool v0 = c0 < g.h, v1 = c1 < g.h;
-  const int64_t base = (int64_t)blockIdx.y * L * g.hp;
-  const float2 zero = make_float2(0.f, 0.f);
-  CPair v[8];
-#pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.hp;
-    v[u] = cpack(v0 ? W[r + c0] : zero, v1 ? W[r + c1] : zero);
+struct PY {
+  static constexpr int B = 16 < 8192 / L ? 16 : 8192 / L;
+  static constexpr int PB = B / 2;
+  static constexpr int TPC = L / 8;
+  static constexpr int THREADS = TPC * PB;
+  static constexpr int RB = PB * (int)sizeof(CPair);
+  static constexpr int R = RB >= 128 ? 1 : 128 / RB;
+  __device__ static __forceinline__ int row(int i) {
+    return i ^ ((i >> 3) & (R - 1));
   }
-  const int rb = Q::rd_base(t, p);
-  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
-             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, -1);
-#pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.hp;
-    if (v0) W[r + c0] = clane0(v[u]);
-    if (v1) W[r + c1] = clane1(v[u]);
+  static constexpr bool kFastRead = (TPC / 8) % R == 0;
+  __device__ static __forceinline__ int rd_base(int t, int p) {
+    return kFastRead ? row(t) * PB + p : 0;
+  }
+  __device__ static __forceinline__ int rd(int base, int t, int p, int u) {
+    return kFastRead ? base + u * TPC * PB : row(t + TPC * u) * PB + p;
+  }
+  static constexpr size_t smem = (size_t)L * PB * sizeof(CPair);
+};
+
+__device__ __forceinline__ CPair load_pair(const float2 *p) {
+  const float4 q = *reinterpret_cast<const float4 *>(p);
+  return cpack(make_float2(q.x, q.y), make_float2(q.z, q.w));
+}
+__device__ __forceinline__ void store_pair(float2 *p, const CPair &v, bool v0,
+                                           bool v1) {
+  if (v1) {
+    const float2 a = clane0(v), b = clane1(v);
+    *reinterpret_cast<float4 *>(p) = make_float4(a.x, a.y, b.x, b.y);
+  } else if (v0) {
+    *p = clane0(v);
   }
 }
 
 template <int L>
-__global__ void __launch_bounds__(PP<L>::THREADS)
-    k_yinv_pp(const float2 *__restrict__ Wr, float2 *__restrict__ Wry,
-              FusedGeom g, const float2 *__restrict__ taby) {
-  using Q = PP<L>;
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_yfwd_pp(float2 *__restrict__ W, FusedGeom g,
+              const float2 *__restrict__ taby) {
+  using Q = PY<L>;
   extern __shared__ unsigned char smem_raw[];
   CPair *ex = reinterpret_cast<CPair *>(smem_raw);
   const int t = threadIdx.x / Q::PB;
   const int p = threadIdx.x - t * Q::PB;
-  const int c0 = blockIdx.x * Q::B + p, c1 = c0 + Q::PB;
-  const bool v0 = c0 < g.h, v1 = c1 < g.h;
-  const int ri = blockIdx.y;
-  const int64_t base = (int64_t)ri * L * g.hp;
-  const float2 zero = make_float2(0.f, 0.f);
+  const int c0 = blockIdx.x * Q::B + 2 * p;
+  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
+  const int64_t base = (int64_t)blockIdx.y * L * g.hp + c0;
   CPair v[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int64_t r = base + (int64_t)(t + Q::TPC * u) * g.hp;
-    v[u] = cpack(v0 ? Wr[r + c0] : zero, v1 ? Wr[r + c1] : zero);
-  }
+  for (int u = 0; u < 8; ++u)
+    v[u] = load_pair(W + base + (int64_t)(t + Q::TPC * u) * g.hp);
+  const int rb = Q::rd_base(t, p);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
+             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, -1);
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    store_pair(W + base + (int64_t)(t + Q::TPC * u) * g.hp, v[u], v0, v1);
+}
+
+template <int L>
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_yinv_pp(const float2 *__restrict__ Wr, float2 *__restrict__ Wry,
+              FusedGeom g, const float2 *__restrict__ taby) {
+  using Q = PY<L>;
+  extern __shared__ unsigned char smem_raw[];
+  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  const int t = threadIdx.x / Q::PB;
+  const int p = threadIdx.x - t * Q::PB;
+  const int c0 = blockIdx.x * Q::B + 2 * p;
+  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
+  const int ri = blockIdx.y;
+  const int64_t base = (int64_t)ri * L * g.hp + c0;
+  CPair v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    v[u] = load_pair(Wr + base + (int64_t)(t + Q::TPC * u) * g.hp);
   const int rb = Q::rd_base(t, p);
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
              [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, +1);
-  const int64_t obase = (int64_t)ri * g.rs * g.hp;
+  const int64_t obase = (int64_t)ri * g.rs * g.hp + c0;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
-    for (int rj = (y + g.ro) % L; rj < g.rs; rj += L) {
-      if (v0) Wry[obase + (int64_t)rj * g.hp + c0] = clane0(v[u]);
-      if (v1) Wry[obase + (int64_t)rj * g.hp + c1] = clane1(v[u]);
-    }
+    for (int rj = (y + g.ro) % L; rj < g.rs; rj += L)
+      store_pair(Wry + obase + (int64_t)rj * g.hp, v[u], v0, v1);
   }
 }
 
@@ -1237,13 +1266,16 @@ void FusedSurvey::yfwd(cudaStream_t s) {
   if (is_p2(g.n1)) {
     with_p2(g.n1, [&]<int L>() {
       using Q = P2<T, L>;
-      dim3 grid((g.h + Q::B - 1) / Q::B, g.n0);
-      if constexpr (std::is_same_v<T, float>)
-        k_yfwd_pp<L><<<grid, PP<L>::THREADS, p2_col_smem<T, L>(), s>>>(
-            W.as<float2>(), g, taby.as<float2>());
-      else
+      if constexpr (std::is_same_v<T, float>) {
+        using Y = PY<L>;
+        dim3 grid((g.h + Y::B - 1) / Y::B, g.n0);
+        k_yfwd_pp<L><<<grid, Y::THREADS, Y::smem, s>>>(W.as<float2>(), g,
+                                                        taby.as<float2>());
+      } else {
+        dim3 grid((g.h + Q::B - 1) / Q::B, g.n0);
         k_yfwd_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), g, taby.as<C2<T>>());
+      }
     });
     FC_LAUNCH_CHECK();
     return;
@@ -1310,13 +1342,16 @@ void FusedSurvey::yinv(cudaStream_t s) {
   if (is_p2(g.n1)) {
     with_p2(g.n1, [&]<int L>() {
       using Q = P2<T, L>;
-      dim3 grid((g.h + Q::B - 1) / Q::B, g.rs);
-      if constexpr (std::is_same_v<T, float>)
-        k_yinv_pp<L><<<grid, PP<L>::THREADS, p2_col_smem<T, L>(), s>>>(
+      if constexpr (std::is_same_v<T, float>) {
+        using Y = PY<L>;
+        dim3 grid((g.h + Y::B - 1) / Y::B, g.rs);
+        k_yinv_pp<L><<<grid, Y::THREADS, Y::smem, s>>>(
             Wr.as<float2>(), Wry.as<float2>(), g, taby.as<float2>());
-      else
+      } else {
+        dim3 grid((g.h + Q::B - 1) / Q::B, g.rs);
         k_yinv_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             Wr.as<C2<T>>(), Wry.as<C2<T>>(), g, taby.as<C2<T>>());
+      }
     });
     FC_LAUNCH_CHECK();
     return;
