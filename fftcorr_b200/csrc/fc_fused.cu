@@ -116,6 +116,33 @@ __device__ __forceinline__ float row_weight(const RowPoly &r, float D,
   return r.ell == 2 ? D * poly * ir2 : D * poly * (ir2 * ir2);
 }
 
+// The row polynomial of an (ell, m) term has only the powers of z of one
+// parity up to ell - |m| (spherical_harmonics.h:100-176): its form is one
+// of five (POLY, below), chosen once per thread instead of a full Horner
+// evaluation per cell.
+//   0: c0    1: c1 z    2: c0 + c2 z^2    3: (c1 + c3 z^2) z
+//   4: c0 + (c2 + c4 z^2) z^2
+__host__ __device__ __forceinline__ int row_poly_form(int ell, int m) {
+  const int a = m < 0 ? -m : m;
+  if (ell == 2) return a == 2 ? 0 : a == 1 ? 1 : 2;
+  return a == 4 ? 0 : a == 3 ? 1 : a == 2 ? 2 : a == 1 ? 3 : 4;
+}
+
+template <int POLY, int ELL>
+__device__ __forceinline__ float row_weight_form(const RowPoly &r, float D,
+                                                 float z) {
+  const float z2 = z * z;
+  float poly;
+  if constexpr (POLY == 0) poly = r.c[0];
+  else if constexpr (POLY == 1) poly = r.c[1] * z;
+  else if constexpr (POLY == 2) poly = r.c[2] * z2 + r.c[0];
+  else if constexpr (POLY == 3) poly = (r.c[3] * z2 + r.c[1]) * z;
+  else poly = (r.c[4] * z2 + r.c[2]) * z2 + r.c[0];
+  const float ir2 = __fdividef(1.0f, r.rxy2 + z2 + 1e-20f);
+  if constexpr (ELL == 2) return D * poly * ir2;
+  else return D * poly * (ir2 * ir2);
+}
+
 __device__ __forceinline__ RowPoly load_row_poly(const float4 *__restrict__ tab,
                                                  int64_t row,
                                                  const YlmParams &p) {
@@ -893,21 +920,54 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
     zt = (float)(z0 + (2 * t) * 1.0);
   }
   const float2 zero = make_float2(0.f, 0.f);
-  CPairS v[8];
+  float2 a[8], b[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int jj = t + Q::TPC * u;
-    float2 a = v0 ? src0[jj] : zero;
-    float2 b = v1 ? src1[jj] : zero;
-    if constexpr (WEIGHT) {
-      const float zu = zt + (float)(2 * Q::TPC * u);
-      a.x = row_weight(rp0, a.x, zu);
-      a.y = row_weight(rp0, a.y, zu + 1.0f);
-      b.x = row_weight(rp1, b.x, zu);
-      b.y = row_weight(rp1, b.y, zu + 1.0f);
-    }
-    v[u] = cpack_s(a, b);
+    a[u] = v0 ? src0[jj] : zero;
+    b[u] = v1 ? src1[jj] : zero;
   }
+  if constexpr (WEIGHT) {
+    // One uniform branch per thread picks the weight's form.
+    auto weigh = [&](auto poly, auto ellc) {
+      constexpr int POLY = decltype(poly)::value, ELL = decltype(ellc)::value;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const float zu = zt + (float)(2 * Q::TPC * u);
+        a[u].x = row_weight_form<POLY, ELL>(rp0, a[u].x, zu);
+        a[u].y = row_weight_form<POLY, ELL>(rp0, a[u].y, zu + 1.0f);
+        b[u].x = row_weight_form<POLY, ELL>(rp1, b[u].x, zu);
+        b[u].y = row_weight_form<POLY, ELL>(rp1, b[u].y, zu + 1.0f);
+      }
+    };
+    using std::integral_constant;
+    using I2 = integral_constant<int, 2>;
+    using I4 = integral_constant<int, 4>;
+    if (p.ell == 0) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        a[u] = make_float2(a[u].x * rp0.value0, a[u].y * rp0.value0);
+        b[u] = make_float2(b[u].x * rp1.value0, b[u].y * rp1.value0);
+      }
+    } else if (p.ell == 2) {
+      switch (row_poly_form(2, p.m)) {
+        case 0: weigh(integral_constant<int, 0>(), I2()); break;
+        case 1: weigh(integral_constant<int, 1>(), I2()); break;
+        default: weigh(integral_constant<int, 2>(), I2()); break;
+      }
+    } else {
+      switch (row_poly_form(4, p.m)) {
+        case 0: weigh(integral_constant<int, 0>(), I4()); break;
+        case 1: weigh(integral_constant<int, 1>(), I4()); break;
+        case 2: weigh(integral_constant<int, 2>(), I4()); break;
+        case 3: weigh(integral_constant<int, 3>(), I4()); break;
+        default: weigh(integral_constant<int, 4>(), I4()); break;
+      }
+    }
+  }
+  CPairS v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) v[u] = cpack_s(a[u], b[u]);
   auto exf = [&](int i) { return &ex[pb * RP + i + (i >> 3)]; };
   reg_fft<L>(v, t, exf, tabz, -1, 2);
 #pragma unroll
@@ -915,22 +975,31 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   __syncthreads();
   float2 *dst0 = W + row0 * g.hp;
   float2 *dst1 = W + row1 * g.hp;
+  // Real-to-complex split, outputs k and L - k together: with
+  // e = (Z_k + conj Z_{L-k}) / 2 and o = -i (Z_k - conj Z_{L-k}) / 2,
+  // X_k = e + o w_k and X_{L-k} = conj(e - o w_k) (w_{L-k} = -conj w_k).
   // Unrolled so the twiddle loads of all outputs issue together.
 #pragma unroll
-  for (int i = 0; i <= L / Q::TPC; ++i) {
+  for (int i = 0; i <= L / 2 / Q::TPC; ++i) {
     const int k = t + Q::TPC * i;
-    if (k > L) break;
-    const CPairS a = *exf(k == L ? 0 : k);
+    if (k > L / 2) break;
+    const CPairS za = *exf(k);
     const CPairS c = cconj(*exf(k == 0 ? 0 : L - k));
     CPairS e, o;
-    e.x = 0.5f * (a.x + c.x);
-    e.y = 0.5f * (a.y + c.y);
-    const CPairS d = csub(a, c);
+    e.x = 0.5f * (za.x + c.x);
+    e.y = 0.5f * (za.y + c.y);
+    const CPairS d = csub(za, c);
     o.x = 0.5f * d.y;
     o.y = -0.5f * d.x;
-    const CPairS r = cadd(e, cmul(o, __ldg(&tabz[k])));
+    const CPairS ow = cmul(o, __ldg(&tabz[k]));
+    const CPairS r = cadd(e, ow);
     if (v0) dst0[k] = clane0(r);
     if (v1) dst1[k] = clane1(r);
+    if (k != L / 2) {
+      const CPairS q = cconj(csub(e, ow));
+      if (v0) dst0[L - k] = clane0(q);
+      if (v1) dst1[L - k] = clane1(q);
+    }
   }
 }
 
