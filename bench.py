@@ -295,14 +295,17 @@ def kernel_profile(job, dD, nD, dR, nR):
 
 
 # DRAM bytes (read + write) per launch of the survey pass kernels at 512^3,
-# FP32-mixed, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
-# of `python bench.py --ngrid 512 --nd 2e6 --nr 1e7 --steps 1 --warmup 1
-# --no-fp64 --no-cpu-baseline`; the pass kernels see the same grid as the
-# full workload (only the catalogs are smaller).  Summaries under profiles/.
+# FP32-mixed, from one ncu capture (dram__bytes.sum.per_second x
+# gpu__time_duration.sum) of `python -m fftcorr_b200.cases survey
+# --precision fp32`, whose passes run on the benchmark's grid and work
+# arrays (profiles/fused_passes_survey512_fp32.md).
 TRAFFIC_PER_LAUNCH_512 = {
-    "zfwd": 1055.39e6,
-    "yfwd": 1064.94e6,
-    "xcorr": 1371.43e6,
+    "zfwd": 1048.8e6,
+    "yfwd": 1063.2e6,
+    "xcorr": 1372.2e6,
+    "xcorr00": 792.8e6,
+    "yinv": 144.4e6,
+    "zinv": 49.1e6,
 }
 
 
@@ -327,8 +330,8 @@ def algorithmic_bytes(family, w, precision, rs, ks):
       xcorr00  the ell = 0 term of an autocorrelation: G in (Nc e) + Wr out
              + k-subgrid as xcorr (its transform is a multiple of G)
       yinv   Wr in (rs N1 h e) + Wry out (rs rs h e)
-      zinv   Wry in (rs rs h e) + r-subgrid weight read and
-             read-modify-write (rs^3 * 24)"""
+      zinv   Wry in (rs rs h e) + r-subgrid weight read (s bytes a cell)
+             and FP64 read-modify-write (rs^3 * (16 + s))"""
     s = 8 if precision == "fp64" else 4
     e = 2 * s
     n0, n1, n2 = w.ngrid
@@ -342,7 +345,7 @@ def algorithmic_bytes(family, w, precision, rs, ks):
         "xcorr": 2 * nc * e + rs * n1 * h * e + kc * (16 + s),
         "xcorr00": nc * e + rs * n1 * h * e + kc * (16 + s),
         "yinv": rs * n1 * h * e + rs * rs * h * e,
-        "zinv": rs * rs * h * e + rs ** 3 * 24,
+        "zinv": rs * rs * h * e + rs ** 3 * (16 + s),
         "weight": n * 8 + n * s,
         "copy_pad": n * 8 + n * s,
         "conj_mul": 3 * nc * e,
@@ -791,7 +794,10 @@ def main():
             fam_roof[fam] = {"achieved_gbs": alg / per / 1e9,
                              "frac": alg / per / 1e9 / peak,
                              "us_per_launch": per * 1e6,
-                             "bytes_per_launch": alg}
+                             "bytes_per_launch": alg,
+                             "traffic": (TRAFFIC_PER_LAUNCH_512.get(fam)
+                                         if tuple(w.ngrid) == (512, 512, 512)
+                                         else None)}
     ours = {k: v for k, v in prof.items()
             if k not in ("r2c", "c2r") and k in fam_roof}
     if ours:
