@@ -594,24 +594,55 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
 #pragma unroll
       for (int u = 0; u < 8; ++u) v[u] = cmulc(v[u], gv[u]);
     }
-    // k-subgrid extraction (see k_xcorr): needs P at arbitrary rows.
+    // k-subgrid extraction (see k_xcorr): needs P at arbitrary rows.  Only
+    // CTAs whose y feeds a k-subgrid row (for either sign of ky) and whose
+    // kz range reaches it stage P in shared memory.
     const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
-    if (ksub != nullptr && kz0 <= oz) {
+    const int jr0 = (yy + oy) % g.n1;
+    const int jr1 = ((oy - yy) % g.n1 + g.n1) % g.n1;
+    if (ksub != nullptr && kz0 <= oz && (jr0 < g.ks1 || jr1 < g.ks1)) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
       __syncthreads();
       if (valid && kzi <= oz) {
-        for (int refl = 0; refl < 2; ++refl) {
-          if (refl == 1 && kzi == 0) continue;
-          const int k = refl == 0 ? kzi + oz : oz - kzi;
-          int j = refl == 0 ? (yy + oy) % g.n1 : ((oy - yy) % g.n1 + g.n1) % g.n1;
-          for (; j < g.ks1; j += g.n1) {
-            for (int i = t; i < g.ks0; i += Q::TPC) {
-              const int x = refl == 0 ? ((i - ox) % L + L) % L
-                                      : ((ox - i) % L + L) % L;
-              const double re = (double)exf(x)->x;
-              const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
-              ksub[cell] += (double)ktab[cell] * re;
+        if (g.ks0 <= 3 * Q::TPC && g.ks1 <= g.n1) {
+          // At most three x rows per thread and one row j per reflection:
+          // each reflection's loads are issued together.
+#pragma unroll
+          for (int refl = 0; refl < 2; ++refl) {
+            const int j = refl == 0 ? jr0 : jr1;
+            if (j >= g.ks1 || (refl == 1 && kzi == 0)) continue;
+            const int k = refl == 0 ? kzi + oz : oz - kzi;
+            size_t cell[3];
+            double acc[3], w[3], re[3];
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+              const int i = t + s * Q::TPC;
+              cell[s] = ((size_t)i * g.ks1 + j) * g.ks2 + k;
+              if (i < g.ks0) {
+                const int x = refl == 0 ? ((i - ox) % L + L) % L
+                                        : ((ox - i) % L + L) % L;
+                re[s] = (double)exf(x)->x;
+                w[s] = (double)ktab[cell[s]];
+                acc[s] = ksub[cell[s]];
+              }
+            }
+#pragma unroll
+            for (int s = 0; s < 3; ++s)
+              if (t + s * Q::TPC < g.ks0) ksub[cell[s]] = acc[s] + w[s] * re[s];
+          }
+        } else {
+          for (int refl = 0; refl < 2; ++refl) {
+            if (refl == 1 && kzi == 0) continue;
+            const int k = refl == 0 ? kzi + oz : oz - kzi;
+            for (int j = refl == 0 ? jr0 : jr1; j < g.ks1; j += g.n1) {
+              for (int i = t; i < g.ks0; i += Q::TPC) {
+                const int x = refl == 0 ? ((i - ox) % L + L) % L
+                                        : ((ox - i) % L + L) % L;
+                const double re = (double)exf(x)->x;
+                const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
+                ksub[cell] += (double)ktab[cell] * re;
+              }
             }
           }
         }
@@ -853,6 +884,32 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 #pragma unroll
   for (int u = 0; u < 8; ++u)
     store_pair(W + base + (int64_t)(t + Q::TPC * u) * g.hp, v[u], v0, v1);
+}
+
+// grid2's x transform in the FP32 form: G = DFT_x(W), the same column
+// pairing as the y passes, with rows N1 * hp elements apart.
+template <int L>
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_xfwd_pp(const float2 *__restrict__ W, float2 *__restrict__ G, FusedGeom g,
+              const float2 *__restrict__ tabx) {
+  using Q = PY<L>;
+  extern __shared__ unsigned char smem_raw[];
+  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  const int t = threadIdx.x / Q::PB;
+  const int p = threadIdx.x - t * Q::PB;
+  const int c0 = blockIdx.x * Q::B + 2 * p;
+  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
+  const int64_t stride = (int64_t)g.n1 * g.hp;
+  const int64_t base = (int64_t)blockIdx.y * g.hp + c0;
+  CPair v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) v[u] = load_pair(W + base + (t + Q::TPC * u) * stride);
+  const int rb = Q::rd_base(t, p);
+  reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
+             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, tabx, -1);
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    store_pair(G + base + (t + Q::TPC * u) * stride, v[u], v0, v1);
 }
 
 template <int L>
@@ -1158,6 +1215,8 @@ void p2_set_limits() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_yinv_pp<L>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_xfwd_pp<L>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, false>,
@@ -1364,7 +1423,12 @@ void FusedSurvey::xcorr(bool product, double *ksub, const void *ktab_v,
     with_p2(g.n0, [&]<int L>() {
       using Q = P2<T, L>;
       dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
-      if (!product)
+      if (!product && std::is_same_v<T, float>) {
+        using Y = PY<L>;
+        dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
+        k_xfwd_pp<L><<<gy, Y::THREADS, Y::smem, s>>>(
+            W.as<float2>(), G.as<float2>(), g, tabx.as<float2>());
+      } else if (!product)
         k_xcorr_p2<T, L, 0><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
             nullptr, T(0));
