@@ -477,20 +477,6 @@ struct ScatterP {
                                  (size_t)(THREADS + 1) * 4;
 };
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-
 
 // Global cell of footprint cell (fx, fy, fz) of a unit at (o0, o1, o2) on a
 // grid at least a footprint wide (one wrap at most per axis).

@@ -217,6 +217,22 @@ struct LaunchShape {
 // partials combined in warp order by warp 0.  Every thread must call it;
 // the result is valid in thread 0.  blockDim.x must be a multiple of 32
 // and at most 1024.
+// Asynchronous global -> shared copies (no registers held while they fly);
+// a thread waits for its own with cp_async_wait_all.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 __device__ __forceinline__ double block_sum(double v, double *smem32) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

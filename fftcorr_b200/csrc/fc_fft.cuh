@@ -430,10 +430,17 @@ __device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
 // every column in the CTA must call this together.
 // rd(u) must return ex(t + TPC * u): kernels pass one that adds constant
 // offsets to a per-thread base instead of recomputing the layout's index.
-template <int L, typename C, typename Tw, typename Ex, typename Rd>
+// before_last() runs once the last exchange is complete, before the last
+// pass: from there on the transform no longer touches shared memory, so a
+// kernel may start asynchronous copies into it.
+struct NoHook {
+  __device__ void operator()() const {}
+};
+template <int L, typename C, typename Tw, typename Ex, typename Rd,
+          typename Hook = NoHook>
 __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex, Rd rd,
                                         const Tw *__restrict__ tab, int sign,
-                                        int tab_scale = 1) {
+                                        int tab_scale = 1, Hook before_last = {}) {
   constexpr int TPC = L / 8;
   // Number of radix-8 passes and the leading radix (1, 2 or 4).
   constexpr int LOG = __builtin_ctz(L);
@@ -485,6 +492,7 @@ __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex, Rd rd,
   }
 #pragma unroll
   for (int p = 0; p < P8; ++p) {
+    if (p + 1 == P8) before_last();
     const int k = t & (Ns - 1);
     if (Ns > 1) r8_twiddle(v, k, (L / (8 * Ns)) * tab_scale, tab, sign);
     Dft<8, C>::run(v, sign);

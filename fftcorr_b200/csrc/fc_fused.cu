@@ -799,9 +799,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
 // pair as CPair (packed two-lane instructions), the z pass as CPairS
 // (one-lane instructions), whichever measured faster for the pass.
 // Thread (t, p) holds columns p and p + PB of the CTA's B, so each global
-// access of a warp stays contiguous per row.  (The x pass keeps one column
-// per thread: with its second input stream and inverse transform, two
-// columns per thread cost it more in occupancy than they save.)
+// access of a warp stays contiguous per row.  (The FP32 x passes pair
+// adjacent columns like the y passes, below.)
 template <int L>
 struct PP {
   static constexpr int B = P2<float, L>::B;
@@ -910,6 +909,139 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 #pragma unroll
   for (int u = 0; u < 8; ++u)
     store_pair(G + base + (t + Q::TPC * u) * stride, v[u], v0, v1);
+}
+
+// The FP32 x pass of one (ell, m) term with the same column pairing.
+// MODE 1: P = DFT_x(W) conj(G); MODE 2 (ell = 0 of an autocorrelation):
+// P = w00 |G|^2 with no forward transform (see k_xcorr_p2).  Then the
+// k-subgrid extraction and the inverse transform, stored only at the
+// r-subgrid's rows.  G is read after the forward transform, so a thread
+// holds one pair of columns at a time and two CTAs fit an SM; the other
+// CTA's warps cover those loads.
+template <int L, int MODE>
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_xcorr_pp(const float2 *__restrict__ W, const float2 *__restrict__ G,
+               float2 *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
+               const float2 *__restrict__ tabx, const float *__restrict__ ktab,
+               float w00) {
+  using Q = PY<L>;
+  extern __shared__ unsigned char smem_raw[];
+  CPair *ex = reinterpret_cast<CPair *>(smem_raw);
+  const int t = threadIdx.x / Q::PB;
+  const int p = threadIdx.x - t * Q::PB;
+  const int cb = blockIdx.x * Q::B;
+  const int c0 = cb + 2 * p;
+  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
+  const int yy = blockIdx.y;
+  const int64_t stride = (int64_t)g.n1 * g.hp;
+  const int64_t base = (int64_t)yy * g.hp + c0;
+  auto exf = [&](int i) { return &ex[Q::row(i) * Q::PB + p]; };
+  const int rb = Q::rd_base(t, p);
+  auto exr = [&](int u) { return &ex[Q::rd(rb, t, p, u)]; };
+  CPair v[8];
+  if constexpr (MODE == 2) {
+    const float2 w = f2splat(w00);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const CPair q = load_pair(G + base + (t + Q::TPC * u) * stride);
+      v[u].x = w * __ffma2_rn(q.x, q.x, q.y * q.y);
+      v[u].y = f2splat(0.f);
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      v[u] = load_pair(W + base + (t + Q::TPC * u) * stride);
+    // G's pairs are copied into this thread's own exchange slots while the
+    // last pass of the forward transform computes.  A slot then holds the
+    // two columns as stored in memory, (re, im) of each, so it is read back
+    // with load_pair like a global pair.
+    reg_fft<L>(v, t, exf, exr, tabx, -1, 1, [&] {
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        cp_async16(exr(u), G + base + (t + Q::TPC * u) * stride);
+    });
+    cp_async_wait_all();
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      v[u] = cmulc(v[u], load_pair(reinterpret_cast<const float2 *>(exr(u))));
+  }
+  // k-subgrid extraction, as in k_xcorr_p2, for both columns of the pair.
+  const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
+  const int jr0 = (yy + oy) % g.n1;
+  const int jr1 = ((oy - yy) % g.n1 + g.n1) % g.n1;
+  if (ksub != nullptr && cb <= oz && (jr0 < g.ks1 || jr1 < g.ks1)) {
+    // P goes through shared memory and is read back afterwards, so the
+    // registers of the pair are free while the extraction runs.
+#pragma unroll
+    for (int u = 0; u < 8; ++u) *exr(u) = v[u];
+    __syncthreads();
+    if (c0 <= oz) {
+      if (g.ks0 <= 3 * Q::TPC && g.ks1 <= g.n1) {
+#pragma unroll
+        for (int refl = 0; refl < 2; ++refl) {
+          const int j = refl == 0 ? jr0 : jr1;
+          if (j >= g.ks1) continue;
+          size_t cell[3][2];
+          double acc[3][2], w[3][2], re[3][2];
+          bool on[3][2];
+#pragma unroll
+          for (int s = 0; s < 3; ++s) {
+            const int i = t + s * Q::TPC;
+            const int x = refl == 0 ? ((i - ox) % L + L) % L : ((ox - i) % L + L) % L;
+#pragma unroll
+            for (int ln = 0; ln < 2; ++ln) {
+              const int kzi = c0 + ln;
+              on[s][ln] = i < g.ks0 && kzi <= oz && !(refl == 1 && kzi == 0);
+              const int k = refl == 0 ? kzi + oz : oz - kzi;
+              cell[s][ln] = ((size_t)i * g.ks1 + j) * g.ks2 + k;
+              if (on[s][ln]) {
+                re[s][ln] = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
+                w[s][ln] = (double)ktab[cell[s][ln]];
+                acc[s][ln] = ksub[cell[s][ln]];
+              }
+            }
+          }
+#pragma unroll
+          for (int s = 0; s < 3; ++s)
+#pragma unroll
+            for (int ln = 0; ln < 2; ++ln)
+              if (on[s][ln]) ksub[cell[s][ln]] = acc[s][ln] + w[s][ln] * re[s][ln];
+        }
+      } else {
+        for (int ln = 0; ln < 2; ++ln) {
+          const int kzi = c0 + ln;
+          if (kzi > oz) continue;
+          for (int refl = 0; refl < 2; ++refl) {
+            if (refl == 1 && kzi == 0) continue;
+            const int k = refl == 0 ? kzi + oz : oz - kzi;
+            for (int j = refl == 0 ? jr0 : jr1; j < g.ks1; j += g.n1) {
+              for (int i = t; i < g.ks0; i += Q::TPC) {
+                const int x = refl == 0 ? ((i - ox) % L + L) % L
+                                        : ((ox - i) % L + L) % L;
+                const double re = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
+                const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
+                ksub[cell] += (double)ktab[cell] * re;
+              }
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = *exr(u);
+    __syncthreads();
+  } else if constexpr (MODE == 1) {
+    // Every thread has read G from its slots before the inverse transform's
+    // first exchange writes over them.
+    __syncthreads();
+  }
+  reg_fft<L>(v, t, exf, exr, tabx, +1);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int x = t + Q::TPC * u;
+    for (int ri = (x + g.ro) % L; ri < g.rs; ri += L)
+      store_pair(out + base + ri * stride, v[u], v0, v1);
+  }
 }
 
 template <int L>
@@ -1217,6 +1349,10 @@ void p2_set_limits() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_xfwd_pp<L>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_xcorr_pp<L, 1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_xcorr_pp<L, 2>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, false>,
@@ -1432,7 +1568,13 @@ void FusedSurvey::xcorr(bool product, double *ksub, const void *ktab_v,
         k_xcorr_p2<T, L, 0><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
             nullptr, T(0));
-      else
+      else if constexpr (std::is_same_v<T, float>) {
+        using Y = PY<L>;
+        dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
+        k_xcorr_pp<L, 1><<<gy, Y::THREADS, Y::smem, s>>>(
+            W.as<float2>(), G.as<float2>(), Wr.as<float2>(), ksub, g,
+            tabx.as<float2>(), ktab, 0.f);
+      } else
         k_xcorr_p2<T, L, 1><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g,
             tabx.as<C2<T>>(), ktab, T(0));
@@ -1462,10 +1604,18 @@ void FusedSurvey::xcorr00(double *ksub, const void *ktab_v, double w00,
   const T *ktab = static_cast<const T *>(ktab_v);
   with_p2(g.n0, [&]<int L>() {
     using Q = P2<T, L>;
-    dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
-    k_xcorr_p2<T, L, 2><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
-        nullptr, G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g, tabx.as<C2<T>>(), ktab,
-        (T)w00);
+    if constexpr (std::is_same_v<T, float>) {
+      using Y = PY<L>;
+      dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
+      k_xcorr_pp<L, 2><<<gy, Y::THREADS, Y::smem, s>>>(
+          nullptr, G.as<float2>(), Wr.as<float2>(), ksub, g, tabx.as<float2>(),
+          ktab, (float)w00);
+    } else {
+      dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
+      k_xcorr_p2<T, L, 2><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
+          nullptr, G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g, tabx.as<C2<T>>(),
+          ktab, (T)w00);
+    }
   });
   FC_LAUNCH_CHECK();
 }
