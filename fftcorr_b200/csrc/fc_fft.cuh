@@ -33,8 +33,16 @@ __device__ __forceinline__ float2 f2splat(float s) { return make_float2(s, s); }
 __device__ __forceinline__ float2 operator+(float2 a, float2 b) {
   return __fadd2_rn(a, b);
 }
+// Packed subtract (PTX sub.rn.f32x2; there is no intrinsic for it): one
+// rounding of a - b per lane, with no register pair of -1 constants.
 __device__ __forceinline__ float2 operator-(float2 a, float2 b) {
-  return __ffma2_rn(b, f2splat(-1.f), a);  // b * -1 is exact
+  unsigned long long ra, rb, rd;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(rd));
+  return r;
 }
 __device__ __forceinline__ float2 operator-(float2 a) {
   return make_float2(-a.x, -a.y);

@@ -524,7 +524,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
-    for (int rj = (y + g.ro) % L; rj < g.rs; rj += L)
+    for (int rj = (y + g.ro) & (L - 1); rj < g.rs; rj += L)
       Wry[obase + (int64_t)rj * g.hp] = v[u];
   }
 }
@@ -620,8 +620,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
               const int i = t + s * Q::TPC;
               cell[s] = ((size_t)i * g.ks1 + j) * g.ks2 + k;
               if (i < g.ks0) {
-                const int x = refl == 0 ? ((i - ox) % L + L) % L
-                                        : ((ox - i) % L + L) % L;
+                const int x = refl == 0 ? (i - ox) & (L - 1)
+                                        : (ox - i) & (L - 1);
                 re[s] = (double)exf(x)->x;
                 w[s] = (double)ktab[cell[s]];
                 acc[s] = ksub[cell[s]];
@@ -637,8 +637,8 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
             const int k = refl == 0 ? kzi + oz : oz - kzi;
             for (int j = refl == 0 ? jr0 : jr1; j < g.ks1; j += g.n1) {
               for (int i = t; i < g.ks0; i += Q::TPC) {
-                const int x = refl == 0 ? ((i - ox) % L + L) % L
-                                        : ((ox - i) % L + L) % L;
+                const int x = refl == 0 ? (i - ox) & (L - 1)
+                                        : (ox - i) & (L - 1);
                 const double re = (double)exf(x)->x;
                 const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
                 ksub[cell] += (double)ktab[cell] * re;
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const int x = t + Q::TPC * u;
-        for (int ri = (x + g.ro) % L; ri < g.rs; ri += L)
+        for (int ri = (x + g.ro) & (L - 1); ri < g.rs; ri += L)
           out[obase + ri * stride] = v[u];
       }
     }
@@ -987,7 +987,7 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 #pragma unroll
           for (int s = 0; s < 3; ++s) {
             const int i = t + s * Q::TPC;
-            const int x = refl == 0 ? ((i - ox) % L + L) % L : ((ox - i) % L + L) % L;
+            const int x = refl == 0 ? (i - ox) & (L - 1) : (ox - i) & (L - 1);
 #pragma unroll
             for (int ln = 0; ln < 2; ++ln) {
               const int kzi = c0 + ln;
@@ -1016,8 +1016,8 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
             const int k = refl == 0 ? kzi + oz : oz - kzi;
             for (int j = refl == 0 ? jr0 : jr1; j < g.ks1; j += g.n1) {
               for (int i = t; i < g.ks0; i += Q::TPC) {
-                const int x = refl == 0 ? ((i - ox) % L + L) % L
-                                        : ((ox - i) % L + L) % L;
+                const int x = refl == 0 ? (i - ox) & (L - 1)
+                                        : (ox - i) & (L - 1);
                 const double re = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
                 const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
                 ksub[cell] += (double)ktab[cell] * re;
@@ -1039,7 +1039,7 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int x = t + Q::TPC * u;
-    for (int ri = (x + g.ro) % L; ri < g.rs; ri += L)
+    for (int ri = (x + g.ro) & (L - 1); ri < g.rs; ri += L)
       store_pair(out + base + ri * stride, v[u], v0, v1);
   }
 }
@@ -1068,7 +1068,7 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
-    for (int rj = (y + g.ro) % L; rj < g.rs; rj += L)
+    for (int rj = (y + g.ro) & (L - 1); rj < g.rs; rj += L)
       store_pair(Wry + obase + (int64_t)rj * g.hp, v[u], v0, v1);
   }
 }
