@@ -826,9 +826,9 @@ struct PP {
 // is 16 where the CTA allows it, so a warp's access covers whole 128-byte
 // row segments.  (Row pitches are multiples of 16 columns, so the pair of
 // the last valid column lies in the padding and is read but never stored.)
-template <int L>
+template <int L, int BW = 16>
 struct PY {
-  static constexpr int B = 16 < 8192 / L ? 16 : 8192 / L;
+  static constexpr int B = BW < 8192 / L ? BW : 8192 / L;
   static constexpr int PB = B / 2;
   static constexpr int TPC = L / 8;
   static constexpr int THREADS = TPC * PB;
@@ -918,13 +918,14 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 // r-subgrid's rows.  G is read after the forward transform, so a thread
 // holds one pair of columns at a time and two CTAs fit an SM; the other
 // CTA's warps cover those loads.
+constexpr int kXB = 16;  // columns per CTA of the FP32 x passes
 template <int L, int MODE>
-__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+__global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREADS)
     k_xcorr_pp(const float2 *__restrict__ W, const float2 *__restrict__ G,
                float2 *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
                const float2 *__restrict__ tabx, const float *__restrict__ ktab,
                float w00) {
-  using Q = PY<L>;
+  using Q = PY<L, kXB>;
   extern __shared__ unsigned char smem_raw[];
   CPair *ex = reinterpret_cast<CPair *>(smem_raw);
   const int t = threadIdx.x / Q::PB;
@@ -1569,7 +1570,7 @@ void FusedSurvey::xcorr(bool product, double *ksub, const void *ktab_v,
             W.as<C2<T>>(), nullptr, G.as<C2<T>>(), nullptr, g, tabx.as<C2<T>>(),
             nullptr, T(0));
       else if constexpr (std::is_same_v<T, float>) {
-        using Y = PY<L>;
+        using Y = PY<L, kXB>;
         dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
         k_xcorr_pp<L, 1><<<gy, Y::THREADS, Y::smem, s>>>(
             W.as<float2>(), G.as<float2>(), Wr.as<float2>(), ksub, g,
@@ -1605,7 +1606,7 @@ void FusedSurvey::xcorr00(double *ksub, const void *ktab_v, double w00,
   with_p2(g.n0, [&]<int L>() {
     using Q = P2<T, L>;
     if constexpr (std::is_same_v<T, float>) {
-      using Y = PY<L>;
+      using Y = PY<L, kXB>;
       dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
       k_xcorr_pp<L, 2><<<gy, Y::THREADS, Y::smem, s>>>(
           nullptr, G.as<float2>(), Wr.as<float2>(), ksub, g, tabx.as<float2>(),
