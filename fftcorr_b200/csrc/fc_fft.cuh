@@ -433,6 +433,31 @@ __device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
   v[7] = cmul(v[7], cmul(w3, w4));
 }
 
+// Outputs 0 and 7 of Dft<8> only (into v[0] and v[7]), by the same
+// operations, for transforms whose later use reads only the first and the
+// last TPC rows.
+template <typename C>
+__device__ __forceinline__ void dft8_edges(C *v, int sign) {
+  using T = typename Real<C>::type;
+  const T h = (T)0.70710678118654752440;
+  const T sg = (T)sign;
+  C a[4], b[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    a[u] = cadd(v[u], v[u + 4]);
+    b[u] = csub(v[u], v[u + 4]);
+  }
+  C t = b[1];
+  b[1].x = h * (t.x - sg * t.y);
+  b[1].y = h * (t.y + sg * t.x);
+  b[2] = cmuli(b[2], sign);
+  t = b[3];
+  b[3].x = h * (-t.x - sg * t.y);
+  b[3].y = h * (-t.y + sg * t.x);
+  v[0] = cadd(cadd(a[0], a[2]), cadd(a[1], a[3]));
+  v[7] = csub(csub(b[0], b[2]), cmuli(csub(b[1], b[3]), sign));
+}
+
 // Transform of one column held in registers (layout above).  ex(i) gives the
 // shared-memory slot of row i of this thread's column; all TPC threads of
 // every column in the CTA must call this together.
@@ -440,7 +465,8 @@ __device__ __forceinline__ void r8_twiddle(C *v, int k, int step,
 // offsets to a per-thread base instead of recomputing the layout's index.
 // before_last() runs once the last exchange is complete, before the last
 // pass: from there on the transform no longer touches shared memory, so a
-// kernel may start asynchronous copies into it.
+// kernel may start asynchronous copies into it.  With edges_only the last
+// pass computes only outputs t and t + 7 TPC (v[0] and v[7]).
 struct NoHook {
   __device__ void operator()() const {}
 };
@@ -448,7 +474,8 @@ template <int L, typename C, typename Tw, typename Ex, typename Rd,
           typename Hook = NoHook>
 __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex, Rd rd,
                                         const Tw *__restrict__ tab, int sign,
-                                        int tab_scale = 1, Hook before_last = {}) {
+                                        int tab_scale = 1, Hook before_last = {},
+                                        bool edges_only = false) {
   constexpr int TPC = L / 8;
   // Number of radix-8 passes and the leading radix (1, 2 or 4).
   constexpr int LOG = __builtin_ctz(L);
@@ -503,7 +530,10 @@ __device__ __forceinline__ void reg_fft(C *v, int t, Ex ex, Rd rd,
     if (p + 1 == P8) before_last();
     const int k = t & (Ns - 1);
     if (Ns > 1) r8_twiddle(v, k, (L / (8 * Ns)) * tab_scale, tab, sign);
-    Dft<8, C>::run(v, sign);
+    if (p + 1 == P8 && edges_only)
+      dft8_edges(v, sign);
+    else
+      Dft<8, C>::run(v, sign);
     if (p + 1 < P8) {
       const int o = (t - k) * 8 + k;
 #pragma unroll

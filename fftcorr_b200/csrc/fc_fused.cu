@@ -1036,7 +1036,18 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
     // first exchange writes over them.
     __syncthreads();
   }
-  reg_fft<L>(v, t, exf, exr, tabx, +1);
+  // Rows x whose r-subgrid row (x + ro) mod L is below rs; when they all lie
+  // in the first and last TPC rows, only outputs u = 0 and 7 are computed.
+  const bool edges = g.ro <= Q::TPC && g.rs - g.ro <= Q::TPC;
+  reg_fft<L>(v, t, exf, exr, tabx, +1, 1, NoHook{}, edges);
+  if (edges) {
+#pragma unroll
+    for (int u = 0; u < 8; u += 7) {
+      const int ri = (t + Q::TPC * u + g.ro) & (L - 1);
+      if (ri < g.rs) store_pair(out + base + ri * stride, v[u], v0, v1);
+    }
+    return;
+  }
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int x = t + Q::TPC * u;
@@ -1063,9 +1074,19 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
   for (int u = 0; u < 8; ++u)
     v[u] = load_pair(Wr + base + (int64_t)(t + Q::TPC * u) * g.hp);
   const int rb = Q::rd_base(t, p);
+  const bool edges = g.ro <= Q::TPC && g.rs - g.ro <= Q::TPC;  // see k_xcorr_pp
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
-             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, +1);
+             [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, +1, 1,
+             NoHook{}, edges);
   const int64_t obase = (int64_t)ri * g.rs * g.hp + c0;
+  if (edges) {
+#pragma unroll
+    for (int u = 0; u < 8; u += 7) {
+      const int rj = (t + Q::TPC * u + g.ro) & (L - 1);
+      if (rj < g.rs) store_pair(Wry + obase + (int64_t)rj * g.hp, v[u], v0, v1);
+    }
+    return;
+  }
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
