@@ -210,8 +210,11 @@ class SurveyJob:
         from fftcorr_b200.correlate import TSC_ALIASED_CORRECTION
         self.fb = fb
         self.w = w
-        self.gA = fb.ConfigSpaceGrid.from_geometry(w.ngrid, w.posmin, w.cell)
-        self.gB = fb.ConfigSpaceGrid.from_geometry(w.ngrid, w.posmin, w.cell)
+        # Grids of the form's precision: the FP32-mixed form's cells are FP32.
+        self.gA = fb.ConfigSpaceGrid.from_geometry(w.ngrid, w.posmin, w.cell,
+                                                   precision=precision)
+        self.gB = fb.ConfigSpaceGrid.from_geometry(w.ngrid, w.posmin, w.cell,
+                                                   precision=precision)
         tsc = fb.DistributionScheme.TRIANGULAR_SHAPED_CLOUD
         self.maA = fb.MassAssignor(self.gA, tsc, False, 0)
         self.maB = fb.MassAssignor(self.gB, tsc, False, 0)

@@ -134,6 +134,10 @@ _SIGNATURES = {
     "fc_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
     "fc_set_device": (ctypes.c_int, [ctypes.c_int]),
     "fc_grid_create": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_double, c_void_pp]),
+    "fc_grid_create_precision": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_double,
+                                                ctypes.c_int, c_void_pp]),
+    "fc_grid_precision": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
+    "fc_grid_device_data": (ctypes.c_int, [ctypes.c_void_p, c_void_pp]),
     "fc_grid_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_grid_clear": (ctypes.c_int, [ctypes.c_void_p]),
     "fc_grid_upload": (ctypes.c_int, [ctypes.c_void_p, c_double_p]),

@@ -7,7 +7,8 @@
 
 survey: a survey Correlator (ell <= 4, rmax 200 / dr 5, kmax 0.3 / dk
 0.005, the benchmark's geometry) autocorrelating a seeded random device
-grid, once to warm up and then --runs times.  periodic: a PeriodicCorrelator
+grid of the same precision (FP32 cells for fp32), once to warm up and then
+--runs times.  periodic: a PeriodicCorrelator
 (ell <= 2) on a seeded random grid, FP32 then FP64, two runs each.  batch:
 six periodic boxes (128^3, 192^3, 256^3; 1M clustered particles each) in one
 CUDA graph, run twice.  assign: TSC mass assignment of seeded uniform
@@ -28,7 +29,7 @@ def _survey(a):
     from fftcorr_b200.correlate import TSC_ALIASED_CORRECTION
     shape = (a.ngrid,) * 3
     posmin, cell = mocks.survey_box(mocks.Sector(), 200.0, shape)
-    grid = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell)
+    grid = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell, precision=a.precision)
     host = np.random.default_rng(1).standard_normal(shape)
     _lib.call("fc_grid_upload", grid.handle, _lib.dptr(host))
     del host

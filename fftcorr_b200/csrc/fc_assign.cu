@@ -332,13 +332,13 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v,
 
 // K-scatter for one colour pass.  Shared memory layout:
 //   acc[F^3] footprint sums | wts[kChunk][3W] | pcell[kChunk] | cstart[513]
-template <int S, typename KeyT>
+template <int S, typename KeyT, typename GT>
 __global__ void __launch_bounds__(kScatterThreads)
     k_scatter(const double *__restrict__ posw, const KeyT *__restrict__ keys,
               const uint32_t *__restrict__ vals,
               const uint32_t *__restrict__ tile_start,
               const uint32_t *__restrict__ tiles, AssignGeom g,
-              double *__restrict__ grid) {
+              GT *__restrict__ grid) {
   constexpr int W = Stencil<S>::W;
   constexpr int OMIN = Stencil<S>::OMIN;
   constexpr int F = kTile + W - 1;
@@ -432,7 +432,8 @@ __global__ void __launch_bounds__(kScatterThreads)
     if (gx < 0) gx += g.n[0];
     if (gy < 0) gy += g.n[1];
     if (gz < 0) gz += g.n[2];
-    grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz] += v;
+    GT &cell = grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz];
+    cell = (GT)((double)cell + v);
   }
 }
 
@@ -493,13 +494,15 @@ __device__ __forceinline__ size_t foot_cell(int fx, int fy, int fz, int o0,
 
 // ranges: this colour's non-empty units (unit, first, end), `count` of
 // them; `next` is this colour's work counter (zero before the pass).
-template <int S, typename KeyT, int TX>
+// GT is the grid's cell type: each footprint cell's FP64 sum for the unit is
+// added to the cell in FP64 and rounded to GT once.
+template <int S, typename KeyT, int TX, typename GT>
 __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
     k_scatter_p(const double *__restrict__ posw, const KeyT *__restrict__ keys,
                 const uint32_t *__restrict__ vals,
                 const uint4 *__restrict__ ranges,
                 const unsigned *__restrict__ count, unsigned *next,
-                AssignGeom g, double *__restrict__ grid) {
+                AssignGeom g, GT *__restrict__ grid) {
   using Q = ScatterP<S, TX>;
   constexpr int W = Q::W;
   constexpr int W3 = Q::W3;
@@ -518,8 +521,8 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
   double *pd = smem;                                     // [C][4]
   double *stab = smem;                                   // [W3][T], after pd
   double *acc = smem + Q::REGION0;                       // [F3]
-  double *gfoot = acc + F3;                              // [F3]
-  int *perm = reinterpret_cast<int *>(gfoot + F3);       // [C]
+  GT *gfoot = reinterpret_cast<GT *>(acc + F3);          // [F3]
+  int *perm = reinterpret_cast<int *>(acc + 2 * F3);     // [C]
   int *wcs = perm + C;                                   // [NW][T]
   int *cstart = wcs + NW * T;                            // [T + 1]
   __shared__ uint4 s_rg;
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
     // colour pass touches these cells.)  The first chunk's wait covers it.
     if (direct) {
       for (int f = h; f < F3; f += T)
-        cp_async8(gfoot + f, grid + foot_cell<OMIN>(f / (FY * FY), (f / FY) % FY,
+        cp_async_cell(gfoot + f, grid + foot_cell<OMIN>(f / (FY * FY), (f / FY) % FY,
                                                     f % FY, o0, o1, o2, g));
     }
 
@@ -689,7 +692,8 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
       }
       if (direct) {
         if (v != 0.0)
-          grid[foot_cell<OMIN>(fx, fy, fz, o0, o1, o2, g)] = gfoot[f] + v;
+          grid[foot_cell<OMIN>(fx, fy, fz, o0, o1, o2, g)] =
+              (GT)((double)gfoot[f] + v);
       } else {
         acc[f] = v;
       }
@@ -715,7 +719,8 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
         if (gx < 0) gx += g.n[0];
         if (gy < 0) gy += g.n[1];
         if (gz < 0) gz += g.n[2];
-        grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz] += v;
+        GT &cell = grid[((size_t)gx * g.n[1] + gy) * g.n[2] + gz];
+        cell = (GT)((double)cell + v);
       }
     }
     if (threadIdx.x == 0) {
@@ -780,20 +785,20 @@ int stencil_width(int scheme, int *omin) {
   }
 }
 
-// Scatter kernel for scheme 0, 1 or 3 and a key type.
-template <typename KeyT>
+// Scatter kernel for scheme 0, 1 or 3, a key type and a cell type.
+template <typename KeyT, typename GT>
 void scatter_p_kernel(int scheme, const void **fn, size_t *smem) {
   switch (scheme) {
     case 0:
-      *fn = (const void *)k_scatter_p<0, KeyT, kUnitX>;
+      *fn = (const void *)k_scatter_p<0, KeyT, kUnitX, GT>;
       *smem = ScatterP<0, kUnitX>::smem;
       break;
     case 1:
-      *fn = (const void *)k_scatter_p<1, KeyT, kUnitX>;
+      *fn = (const void *)k_scatter_p<1, KeyT, kUnitX, GT>;
       *smem = ScatterP<1, kUnitX>::smem;
       break;
     default:
-      *fn = (const void *)k_scatter_p<3, KeyT, kUnitX>;
+      *fn = (const void *)k_scatter_p<3, KeyT, kUnitX, GT>;
       *smem = ScatterP<3, kUnitX>::smem;
       break;
   }
@@ -882,10 +887,14 @@ struct Assignor {
     FC_CUDA(cudaMemsetAsync(counts.get(), 0, counts.bytes(), grid->stream));
     if (scheme != 2) {
       while ((1 << unit_shift) < unit_x * kTile * kTile) ++unit_shift;
-      if (wide_keys)
-        scatter_p_kernel<uint64_t>(scheme, &scatter_fn, &scatter_smem_bytes);
+      if (wide_keys && grid->fp32())
+        scatter_p_kernel<uint64_t, float>(scheme, &scatter_fn, &scatter_smem_bytes);
+      else if (wide_keys)
+        scatter_p_kernel<uint64_t, double>(scheme, &scatter_fn, &scatter_smem_bytes);
+      else if (grid->fp32())
+        scatter_p_kernel<uint32_t, float>(scheme, &scatter_fn, &scatter_smem_bytes);
       else
-        scatter_p_kernel<uint32_t>(scheme, &scatter_fn, &scatter_smem_bytes);
+        scatter_p_kernel<uint32_t, double>(scheme, &scatter_fn, &scatter_smem_bytes);
       scatter_threads = unit_x * 64;
       FC_CUDA(cudaFuncSetAttribute(scatter_fn,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -896,10 +905,16 @@ struct Assignor {
       scatter_ctas = (unsigned)std::max(1, per_sm) * (unsigned)sm_count();
     }
     if (scheme == 2) {
-      FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t>,
+      FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t, double>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)scatter_smem<2>()));
-      FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint64_t>,
+      FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint64_t, double>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)scatter_smem<2>()));
+      FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t, float>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)scatter_smem<2>()));
+      FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint64_t, float>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)scatter_smem<2>()));
     }
@@ -1144,9 +1159,16 @@ struct Assignor {
     for (int c = 0; c < ncolors; ++c) {
       const int64_t nu = color_offsets[c + 1] - color_offsets[c];
       if (nu == 0) continue;
-      k_scatter<2, KeyT><<<(unsigned)nu, kScatterThreads, scatter_smem<2>(),
-                           stream()>>>(src_posw, sk, sv, unit_start.as<uint32_t>(),
-                                       units + color_offsets[c], geom, grid->ptr());
+      if (grid->fp32())
+        k_scatter<2, KeyT, float><<<(unsigned)nu, kScatterThreads,
+                                    scatter_smem<2>(), stream()>>>(
+            src_posw, sk, sv, unit_start.as<uint32_t>(), units + color_offsets[c],
+            geom, static_cast<float *>(grid->raw()));
+      else
+        k_scatter<2, KeyT, double><<<(unsigned)nu, kScatterThreads,
+                                     scatter_smem<2>(), stream()>>>(
+            src_posw, sk, sv, unit_start.as<uint32_t>(), units + color_offsets[c],
+            geom, grid->ptr());
       FC_LAUNCH_CHECK();
     }
     if (!graph_mode) window_timer.stop(stream());
@@ -1174,7 +1196,7 @@ struct Assignor {
         units, nunits, unit_start.as<uint32_t>(), color_off_dev.as<int64_t>(),
         ncolors, counters, unit_ranges.as<uint4>());
     FC_LAUNCH_CHECK();
-    double *gp = grid->ptr();
+    void *gp = grid->raw();
     AssignGeom ga = geom;
     const double *pw = src_posw;
     for (int c = 0; c < ncolors; ++c) {

@@ -229,6 +229,18 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src)
                : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+// One grid cell of either type.
+__device__ __forceinline__ void cp_async_cell(double *dst, const double *src) {
+  cp_async8(dst, src);
+}
+__device__ __forceinline__ void cp_async_cell(float *dst, const float *src) {
+  cp_async4(dst, src);
+}
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }

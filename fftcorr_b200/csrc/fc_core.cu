@@ -83,32 +83,43 @@ __global__ void k_fill(double *a, size_t n, double v) {
     a[i] = v;
 }
 
-__global__ void k_add_scalar(double *a, size_t n, double s) {
+// Grid arithmetic in FP64 per cell, rounded once to the cell type.
+template <typename T>
+__global__ void k_add_scalar(T *a, size_t n, double s) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    a[i] += s;
+    a[i] = (T)((double)a[i] + s);
 }
 
-__global__ void k_multiply_by(double *a, size_t n, double s) {
+template <typename T>
+__global__ void k_multiply_by(T *a, size_t n, double s) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    a[i] *= s;
+    a[i] = (T)((double)a[i] * s);
 }
 
-__global__ void k_axpy(double *y, const double *x, size_t n, double a) {
+template <typename TY, typename TX>
+__global__ void k_axpy(TY *y, const TX *x, size_t n, double a) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    y[i] += a * x[i];
+    y[i] = (TY)((double)y[i] + a * (double)x[i]);
+}
+
+__global__ void k_widen(const float *in, double *out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
 }
 
 // Pass 1 of the deterministic sum/sumsq: block b reduces the grid-stride
 // subsequence it owns in a fixed order.
-__global__ void k_sum_partials(const double *a, size_t n, double *partials) {
+template <typename T>
+__global__ void k_sum_partials(const T *a, size_t n, double *partials) {
   __shared__ double red[32];
   double s = 0.0, q = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    const double v = a[i];
+    const double v = (double)a[i];
     s += v;
     q += v * v;
   }
@@ -144,12 +155,26 @@ void device_fill(double *a, size_t n, double v, cudaStream_t s) {
   FC_LAUNCH_CHECK();
 }
 
-void device_sum_sumsq(const double *a, size_t n, double *scratch,
-                      cudaStream_t s) {
+template <typename T>
+static void sum_sumsq(const T *a, size_t n, double *scratch, cudaStream_t s) {
   // scratch: 2 * kSumBlocks partials followed by the 2 results.
-  k_sum_partials<<<kSumBlocks, 256, 0, s>>>(a, n, scratch);
+  k_sum_partials<T><<<kSumBlocks, 256, 0, s>>>(a, n, scratch);
   FC_LAUNCH_CHECK();
   k_sum_final<<<1, 256, 0, s>>>(scratch, kSumBlocks, scratch + 2 * kSumBlocks);
+  FC_LAUNCH_CHECK();
+}
+void device_sum_sumsq(const double *a, size_t n, double *scratch,
+                      cudaStream_t s) {
+  sum_sumsq(a, n, scratch, s);
+}
+void device_sum_sumsq(const float *a, size_t n, double *scratch,
+                      cudaStream_t s) {
+  sum_sumsq(a, n, scratch, s);
+}
+
+void device_widen(const float *in, double *out, size_t n, cudaStream_t s) {
+  if (n == 0) return;
+  k_widen<<<grid_for(n, 256), 256, 0, s>>>(in, out, n);
   FC_LAUNCH_CHECK();
 }
 
@@ -183,7 +208,10 @@ void device_bytes_add(long long delta) { g_device_bytes += delta; }
 
 // ------------------------------------------------------------- the grid
 
-Grid::Grid(const int shp[3], const double pmin[3], double cell) {
+Grid::Grid(const int shp[3], const double pmin[3], double cell, int prec) {
+  FC_REQUIRE(prec == FC_FP64 || prec == FC_FP32_MIXED, FC_ERR_INVALID,
+             "grid precision must be FC_FP64 or FC_FP32_MIXED");
+  precision = prec;
   for (int i = 0; i < 3; ++i) {
     FC_REQUIRE(shp[i] > 0, FC_ERR_INVALID, "grid shape must be positive");
     shape[i] = shp[i];
@@ -194,7 +222,7 @@ Grid::Grid(const int shp[3], const double pmin[3], double cell) {
   FC_CUDA(cudaGetDevice(&device));
   FC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   try {
-    data.resize(size() * sizeof(double));
+    data.resize(size() * cell_bytes());
     scratch.resize((2 * kSumBlocks + 2) * sizeof(double));
     clear();
   } catch (...) {
@@ -212,7 +240,7 @@ Grid::~Grid() {
 }
 
 void Grid::clear() {
-  FC_CUDA(cudaMemsetAsync(data.get(), 0, size() * sizeof(double), stream));
+  FC_CUDA(cudaMemsetAsync(data.get(), 0, size() * cell_bytes(), stream));
 }
 
 }  // namespace fc
@@ -238,14 +266,26 @@ int fc_set_device(int device) {
   return guard([&] { FC_CUDA(cudaSetDevice(device)); });
 }
 
-int fc_grid_create(const int shape[3], const double posmin[3],
-                   double cell_size, fc_grid **out) {
+int fc_grid_create_precision(const int shape[3], const double posmin[3],
+                             double cell_size, int precision, fc_grid **out) {
   return guard([&] {
     FC_REQUIRE(shape && posmin && out, FC_ERR_INVALID, "null argument");
     *out = nullptr;
-    Grid *g = new Grid(shape, posmin, cell_size);
+    std::unique_ptr<Grid> g(new Grid(shape, posmin, cell_size, precision));
     FC_CUDA(cudaStreamSynchronize(g->stream));
-    *out = reinterpret_cast<fc_grid *>(g);
+    *out = reinterpret_cast<fc_grid *>(g.release());
+  });
+}
+
+int fc_grid_create(const int shape[3], const double posmin[3],
+                   double cell_size, fc_grid **out) {
+  return fc_grid_create_precision(shape, posmin, cell_size, FC_FP64, out);
+}
+
+int fc_grid_precision(const fc_grid *grid, int *precision) {
+  return guard([&] {
+    FC_REQUIRE(precision, FC_ERR_INVALID, "null argument");
+    *precision = as_grid(grid)->precision;
   });
 }
 
@@ -265,6 +305,15 @@ int fc_grid_upload(fc_grid *grid, const double *host) {
   return guard([&] {
     Grid *g = as_grid(grid);
     FC_REQUIRE(host, FC_ERR_INVALID, "null host pointer");
+    if (g->fp32()) {
+      // Rounded once per cell on the host, then copied.
+      std::vector<float> tmp(g->size());
+      for (size_t i = 0; i < tmp.size(); ++i) tmp[i] = (float)host[i];
+      FC_CUDA(cudaMemcpyAsync(g->raw(), tmp.data(), tmp.size() * sizeof(float),
+                              cudaMemcpyHostToDevice, g->stream));
+      FC_CUDA(cudaStreamSynchronize(g->stream));
+      return;
+    }
     FC_CUDA(cudaMemcpyAsync(g->ptr(), host, g->size() * sizeof(double),
                             cudaMemcpyHostToDevice, g->stream));
     FC_CUDA(cudaStreamSynchronize(g->stream));
@@ -275,6 +324,14 @@ int fc_grid_download(const fc_grid *grid, double *host) {
   return guard([&] {
     const Grid *g = as_grid(grid);
     FC_REQUIRE(host, FC_ERR_INVALID, "null host pointer");
+    if (g->fp32()) {
+      std::vector<float> tmp(g->size());
+      FC_CUDA(cudaMemcpyAsync(tmp.data(), g->raw(), tmp.size() * sizeof(float),
+                              cudaMemcpyDeviceToHost, g->stream));
+      FC_CUDA(cudaStreamSynchronize(g->stream));
+      for (size_t i = 0; i < tmp.size(); ++i) host[i] = (double)tmp[i];
+      return;
+    }
     FC_CUDA(cudaMemcpyAsync(host, g->ptr(), g->size() * sizeof(double),
                             cudaMemcpyDeviceToHost, g->stream));
     FC_CUDA(cudaStreamSynchronize(g->stream));
@@ -285,6 +342,13 @@ int fc_grid_device_ptr(const fc_grid *grid, double **device_ptr) {
   return guard([&] {
     FC_REQUIRE(device_ptr, FC_ERR_INVALID, "null argument");
     *device_ptr = as_grid(grid)->ptr();
+  });
+}
+
+int fc_grid_device_data(const fc_grid *grid, void **device_ptr) {
+  return guard([&] {
+    FC_REQUIRE(device_ptr, FC_ERR_INVALID, "null argument");
+    *device_ptr = as_grid(grid)->raw();
   });
 }
 
@@ -305,7 +369,11 @@ int fc_grid_sum(fc_grid *grid, double *sum, double *sumsq) {
   return guard([&] {
     Grid *g = as_grid(grid);
     double *scr = g->scratch.as<double>();
-    device_sum_sumsq(g->ptr(), g->size(), scr, g->stream);
+    if (g->fp32())
+      device_sum_sumsq(static_cast<const float *>(g->raw()), g->size(), scr,
+                       g->stream);
+    else
+      device_sum_sumsq(g->ptr(), g->size(), scr, g->stream);
     double res[2];
     FC_CUDA(cudaMemcpyAsync(res, scr + 2 * kSumBlocks, sizeof(res),
                             cudaMemcpyDeviceToHost, g->stream));
@@ -318,8 +386,12 @@ int fc_grid_sum(fc_grid *grid, double *sum, double *sumsq) {
 int fc_grid_add_scalar(fc_grid *grid, double s) {
   return guard([&] {
     Grid *g = as_grid(grid);
-    k_add_scalar<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
-        g->ptr(), g->size(), s);
+    if (g->fp32())
+      k_add_scalar<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
+          static_cast<float *>(g->raw()), g->size(), s);
+    else
+      k_add_scalar<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
+          g->ptr(), g->size(), s);
     FC_LAUNCH_CHECK();
     FC_CUDA(cudaStreamSynchronize(g->stream));
   });
@@ -328,8 +400,12 @@ int fc_grid_add_scalar(fc_grid *grid, double s) {
 int fc_grid_multiply_by(fc_grid *grid, double s) {
   return guard([&] {
     Grid *g = as_grid(grid);
-    k_multiply_by<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
-        g->ptr(), g->size(), s);
+    if (g->fp32())
+      k_multiply_by<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
+          static_cast<float *>(g->raw()), g->size(), s);
+    else
+      k_multiply_by<<<grid_for(g->size(), 256), 256, 0, g->stream>>>(
+          g->ptr(), g->size(), s);
     FC_LAUNCH_CHECK();
     FC_CUDA(cudaStreamSynchronize(g->stream));
   });
@@ -348,8 +424,20 @@ int fc_grid_axpy(fc_grid *y, double a, const fc_grid *x) {
     cudaEventRecord(ev, gx->stream);
     cudaStreamWaitEvent(gy->stream, ev, 0);
     cudaEventDestroy(ev);
-    k_axpy<<<grid_for(gy->size(), 256), 256, 0, gy->stream>>>(
-        gy->ptr(), gx->ptr(), gy->size(), a);
+    const unsigned nb = grid_for(gy->size(), 256);
+    const size_t n = gy->size();
+    float *y32 = static_cast<float *>(gy->raw());
+    const float *x32 = static_cast<const float *>(gx->raw());
+    double *y64 = static_cast<double *>(gy->raw());
+    const double *x64 = static_cast<const double *>(gx->raw());
+    if (gy->fp32() && gx->fp32())
+      k_axpy<<<nb, 256, 0, gy->stream>>>(y32, x32, n, a);
+    else if (gy->fp32())
+      k_axpy<<<nb, 256, 0, gy->stream>>>(y32, x64, n, a);
+    else if (gx->fp32())
+      k_axpy<<<nb, 256, 0, gy->stream>>>(y64, x32, n, a);
+    else
+      k_axpy<<<nb, 256, 0, gy->stream>>>(y64, x64, n, a);
     FC_LAUNCH_CHECK();
     FC_CUDA(cudaStreamSynchronize(gy->stream));
   });

@@ -76,15 +76,15 @@ __global__ void k_weight(const double *__restrict__ rho, T *__restrict__ work,
 
 // copy_into_padded_array (array_ops.cc:35-53), with an optional shift and a
 // precision cast.
-template <typename T>
-__global__ void k_copy_pad(const double *__restrict__ rho, T *__restrict__ work,
+template <typename TI, typename T>
+__global__ void k_copy_pad(const TI *__restrict__ rho, T *__restrict__ work,
                            int n0, int n1, int n2, int n2p, double shift) {
   const size_t nrows = (size_t)n0 * n1;
   for (size_t row = blockIdx.x; row < nrows; row += gridDim.x) {
-    const double *src = rho + row * n2;
+    const TI *src = rho + row * n2;
     T *dst = work + row * n2p;
     for (int k = threadIdx.x; k < n2; k += blockDim.x)
-      dst[k] = (T)(src[k] - shift);
+      dst[k] = (T)((double)src[k] - shift);
   }
 }
 
@@ -633,12 +633,19 @@ struct Correlator {
   }
 
   template <typename T>
-  void copy_pad(const double *rho, double shift) {
+  void copy_pad(Density d, double shift) {
     Profiler::Scope ps(&prof, stream, "copy_pad");
     const size_t nrows = (size_t)geo.shape[0] * geo.shape[1];
-    k_copy_pad<T><<<rows_grid(nrows), row_threads(geo.shape[2]), 0, stream>>>(
-        rho, work.as<T>(), geo.shape[0], geo.shape[1], geo.shape[2], geo.n2p(),
-        shift);
+    if (d.f32)
+      k_copy_pad<float, T><<<rows_grid(nrows), row_threads(geo.shape[2]), 0,
+                             stream>>>(static_cast<const float *>(d.p), work.as<T>(),
+                                       geo.shape[0], geo.shape[1], geo.shape[2],
+                                       geo.n2p(), shift);
+    else
+      k_copy_pad<double, T><<<rows_grid(nrows), row_threads(geo.shape[2]), 0,
+                              stream>>>(static_cast<const double *>(d.p),
+                                        work.as<T>(), geo.shape[0], geo.shape[1],
+                                        geo.shape[2], geo.n2p(), shift);
     FC_LAUNCH_CHECK();
   }
 
@@ -714,26 +721,43 @@ struct Correlator {
   // ----------------------------------------------------------- grid2
 
   template <typename T>
-  void set_grid2_dev(const double *rho) {
+  void set_grid2_dev(Density d) {
     using C = typename Cplx<T>::type;
     if (fused) {
       ProfHook hook(&prof, stream);
       hook.begin("grid2");
-      fused->grid2(fused->prepare_input(rho, stream), stream, kaxes());
+      fused->grid2(fused->prepare_input(d.p, d.f32, stream), stream, kaxes());
       hook.end();
       ++n_fft;
       have_g2 = true;
       return;
     }
     g2.resize(geo.ncomplex() * sizeof(C));
-    copy_pad<T>(rho, shift_for(rho));
+    copy_pad<T>(d, shift_for(d));
     exec_r2c(work.get(), g2.get());
     have_g2 = true;
   }
 
+  // The FP64 cells of a density that accept() has passed through.
+  static const double *fp64_cells(Density d) {
+    FC_REQUIRE(!d.f32, FC_ERR_STATE, "FP32 cells on an FP64 input path");
+    return static_cast<const double *>(d.p);
+  }
+
+  // FP32 cells go straight into the FP32 fused passes and the periodic
+  // copy into the FP32 work grid; every other path reads FP64 cells,
+  // widened here into the staging buffer.
+  Density accept(Density d) {
+    if (!d.f32 || (!fp64() && (fused || kind == FC_PERIODIC))) return d;
+    input.resize(geo.ncells() * sizeof(double));
+    device_widen(static_cast<const float *>(d.p), input.as<double>(),
+                 geo.ncells(), stream);
+    return {input.get(), false};
+  }
+
   // Mean of the grid, removed before FP32 transforms of periodic grids.
-  double shift_for(const double *rho) {
-    (void)rho;
+  double shift_for(Density d) {
+    (void)d;
     return 0.0;
   }
 
@@ -781,9 +805,9 @@ struct Correlator {
 
   // PeriodicCorrelator::correlate_internal (correlator.h:273-357).
   template <typename T>
-  void periodic_run(const double *rho, bool cross) {
+  void periodic_run(Density d, bool cross) {
     const size_t ncells = geo.ncells();
-    copy_pad<T>(rho, 0.0);
+    copy_pad<T>(d, 0.0);
     exec_r2c(work.get(), work.get());
     conj_mul<T>(!cross);
     const double k_rescale = geo.cell * geo.cell * geo.cell / (double)ncells;
@@ -867,12 +891,12 @@ struct Correlator {
   // prepared: the fused passes' input already holds rho (set_grid2 of the
   // same grid has just converted it).
   template <typename T>
-  void survey_run(const double *rho, bool prepared = false) {
+  void survey_run(Density d, bool prepared = false) {
     const size_t ncells = geo.ncells();
     const int maxell = 2 * (geo.nrows - 1);
     if (fused) {
-      const void *in =
-          prepared ? fused->input(rho) : fused->prepare_input(rho, stream);
+      const void *in = prepared ? fused->input(d.p, d.f32)
+                                : fused->prepare_input(d.p, d.f32, stream);
       ProfHook hook(&prof, stream);
       const KAxes ka = kaxes();
       int term = 0;
@@ -892,6 +916,7 @@ struct Correlator {
       }
       return;
     }
+    const double *rho = fp64_cells(d);
     int term = 0;
     for (int ell = 0; ell <= maxell; ell += 2) {
       zero_sub(true, true);
@@ -910,27 +935,28 @@ struct Correlator {
   }
 
   template <typename T>
-  void run_typed(const double *rho, bool cross) {
+  void run_typed(Density d, bool cross) {
     if (kind == FC_PERIODIC) {
       FC_REQUIRE(!cross || have_g2, FC_ERR_STATE,
                  "cross_correlate needs set_grid2 or set_grid2_fft first");
-      periodic_run<T>(rho, cross);
+      periodic_run<T>(d, cross);
     } else {
-      if (!cross) set_grid2_dev<T>(rho);
+      if (!cross) set_grid2_dev<T>(d);
       FC_REQUIRE(have_g2, FC_ERR_STATE,
                  "cross_correlate needs set_grid2 or set_grid2_fft first");
-      survey_run<T>(rho, !cross);
+      survey_run<T>(d, !cross);
     }
   }
 
-  // Enqueues one correlation of a device grid.
-  void enqueue(const double *rho, bool cross) {
+  // Enqueues one correlation of a device density.
+  void enqueue(Density d, bool cross) {
     n_fft = 0;
     FC_CUDA(cudaEventRecord(ev_start, stream));
+    d = accept(d);
     if (fp64())
-      run_typed<double>(rho, cross);
+      run_typed<double>(d, cross);
     else
-      run_typed<float>(rho, cross);
+      run_typed<float>(d, cross);
     FC_CUDA(cudaEventRecord(ev_stop, stream));
     have_result = true;
   }
@@ -949,11 +975,12 @@ struct Correlator {
     return input.as<double>();
   }
 
-  void set_grid2_device(const double *rho) {
+  void set_grid2_device(Density d) {
+    d = accept(d);
     if (fp64())
-      set_grid2_dev<double>(rho);
+      set_grid2_dev<double>(d);
     else
-      set_grid2_dev<float>(rho);
+      set_grid2_dev<float>(d);
   }
 
   void results(double *rbins_out, int *rcounts, double *rhist, double *kbins_out,
@@ -1005,7 +1032,7 @@ void correlator_autocorrelate(Correlator *c, const Grid *g) {
     FC_REQUIRE(g->shape[i] == c->geo.shape[i], FC_ERR_INVALID,
                "grid shape does not match the correlator");
   stream_after(c->stream, g->stream);
-  c->enqueue(g->ptr(), false);
+  c->enqueue(density_of(g), false);
   c->synchronize();
 }
 void correlator_make_deferred(Correlator *c) { c->make_deferred(); }
@@ -1141,7 +1168,7 @@ int fc_corr_set_grid2(fc_correlator *corr, const double *host_grid) {
   return guard([&] {
     Correlator *c = as_corr(corr);
     FC_REQUIRE(host_grid, FC_ERR_INVALID, "null grid");
-    c->set_grid2_device(c->stage_host(host_grid));
+    c->set_grid2_device({c->stage_host(host_grid), false});
     FC_CUDA(cudaStreamSynchronize(c->stream));
   });
 }
@@ -1154,7 +1181,7 @@ int fc_corr_set_grid2_grid(fc_correlator *corr, const fc_grid *grid2) {
       FC_REQUIRE(g->shape[i] == c->geo.shape[i], FC_ERR_INVALID,
                  "grid shape does not match the correlator");
     stream_after(c->stream, g->stream);
-    c->set_grid2_device(g->ptr());
+    c->set_grid2_device(density_of(g));
     FC_CUDA(cudaStreamSynchronize(c->stream));
   });
 }
@@ -1172,7 +1199,7 @@ int fc_corr_autocorrelate(fc_correlator *corr, const double *host_grid) {
   return guard([&] {
     Correlator *c = as_corr(corr);
     FC_REQUIRE(host_grid, FC_ERR_INVALID, "null grid");
-    c->enqueue(c->stage_host(host_grid), false);
+    c->enqueue({c->stage_host(host_grid), false}, false);
     c->synchronize();
   });
 }
@@ -1185,7 +1212,7 @@ int fc_corr_autocorrelate_grid(fc_correlator *corr, const fc_grid *grid) {
       FC_REQUIRE(g->shape[i] == c->geo.shape[i], FC_ERR_INVALID,
                  "grid shape does not match the correlator");
     stream_after(c->stream, g->stream);
-    c->enqueue(g->ptr(), false);
+    c->enqueue(density_of(g), false);
     c->synchronize();
   });
 }
@@ -1198,7 +1225,7 @@ int fc_corr_autocorrelate_grid_async(fc_correlator *corr, const fc_grid *grid) {
       FC_REQUIRE(g->shape[i] == c->geo.shape[i], FC_ERR_INVALID,
                  "grid shape does not match the correlator");
     stream_after(c->stream, g->stream);
-    c->enqueue(g->ptr(), false);
+    c->enqueue(density_of(g), false);
   });
 }
 
@@ -1212,7 +1239,7 @@ int fc_corr_cross_correlate(fc_correlator *corr, const double *host_grid1) {
     FC_REQUIRE(host_grid1, FC_ERR_INVALID, "null grid");
     FC_REQUIRE(c->have_g2, FC_ERR_STATE,
                "cross_correlate needs set_grid2 or set_grid2_fft first");
-    c->enqueue(c->stage_host(host_grid1), true);
+    c->enqueue({c->stage_host(host_grid1), false}, true);
     c->synchronize();
   });
 }
@@ -1227,7 +1254,7 @@ int fc_corr_cross_correlate_grid(fc_correlator *corr, const fc_grid *grid1) {
       FC_REQUIRE(g->shape[i] == c->geo.shape[i], FC_ERR_INVALID,
                  "grid shape does not match the correlator");
     stream_after(c->stream, g->stream);
-    c->enqueue(g->ptr(), true);
+    c->enqueue(density_of(g), true);
     c->synchronize();
   });
 }

@@ -1483,10 +1483,14 @@ void FusedSurvey::set_smem_limits() {
   }
 }
 
-const void *FusedSurvey::prepare_input(const double *rho, cudaStream_t s) {
-  if (fp64_) return rho;
+const void *FusedSurvey::prepare_input(const void *rho, bool f32,
+                                       cudaStream_t s) {
+  FC_REQUIRE(!(fp64_ && f32), FC_ERR_INVALID,
+             "the FP64 passes take FP64 cells");
+  if (fp64_ || f32) return rho;
   const size_t n = (size_t)g.n0 * g.n1 * g.n2;
-  k_to_float<<<grid_for(n, 256), 256, 0, s>>>(rho, rho32.as<float>(), n, 0.0);
+  k_to_float<<<grid_for(n, 256), 256, 0, s>>>(static_cast<const double *>(rho),
+                                              rho32.as<float>(), n, 0.0);
   FC_LAUNCH_CHECK();
   return rho32.get();
 }

@@ -42,13 +42,14 @@ class FusedSurvey {
 
   FusedSurvey(const int shape[3], int rsize, const int kshape[3], bool fp64);
 
-  // The grid in the arithmetic of the passes: rho itself in FP64, an FP32
-  // copy in mixed precision.
-  const void *prepare_input(const double *rho, cudaStream_t s);
-  // What prepare_input(rho) last returned -- valid only while that density
-  // is unchanged.
-  const void *input(const double *rho) const {
-    return fp64_ ? (const void *)rho : rho32.get();
+  // The grid in the arithmetic of the passes: rho itself when its cells
+  // already have the passes' type (f32: FP32 cells, in mixed precision
+  // only), else an FP32 copy of FP64 cells.
+  const void *prepare_input(const void *rho, bool f32, cudaStream_t s);
+  // What prepare_input(rho, f32) last returned -- valid only while that
+  // density is unchanged.
+  const void *input(const void *rho, bool f32) const {
+    return fp64_ || f32 ? rho : rho32.get();
   }
   // G = 3-D DFT of the prepared grid (BaseCorrelator::set_grid2).
   void grid2(const void *rho_in, cudaStream_t s, const KAxes &ka);

@@ -17,12 +17,16 @@ const char *last_error_cstr();
 std::atomic<unsigned long long> &launch_counter();
 
 // ConfigSpaceGrid (cc/grid/config_space_grid.h:10-57): an N0 x N1 x N2
-// row-major FP64 grid resident in HBM, with the geometry that maps survey
-// coordinates onto it.  Work on the grid is ordered on its stream.
+// row-major grid resident in HBM, with the geometry that maps survey
+// coordinates onto it.  Work on the grid is ordered on its stream.  Cells
+// are FP64 (the reference's type) or, for grids made for the FP32-mixed
+// correlators, FP32: mass assignment still sums in FP64 and rounds once per
+// update of a cell, and arithmetic on the grid is done in FP64 per cell.
 struct Grid {
   int shape[3];
   double posmin[3];
   double cell_size;
+  int precision = FC_FP64;  // FC_FP64 or FC_FP32_MIXED (FP32 cells)
   int device = 0;
   cudaStream_t stream = nullptr;
   DeviceBuffer data;
@@ -30,12 +34,28 @@ struct Grid {
   // Expires with the grid, so objects that use it can tell it has gone.
   std::shared_ptr<int> alive = std::make_shared<int>(0);
 
-  Grid(const int shp[3], const double pmin[3], double cell);
+  Grid(const int shp[3], const double pmin[3], double cell,
+       int precision = FC_FP64);
   ~Grid();
   void clear();
   size_t size() const { return (size_t)shape[0] * shape[1] * shape[2]; }
-  double *ptr() const { return data.as<double>(); }
+  bool fp32() const { return precision == FC_FP32_MIXED; }
+  size_t cell_bytes() const { return fp32() ? sizeof(float) : sizeof(double); }
+  void *raw() const { return data.get(); }
+  // The cells of an FP64 grid.
+  double *ptr() const {
+    FC_REQUIRE(!fp32(), FC_ERR_INVALID, "this operation needs an FP64 grid");
+    return data.as<double>();
+  }
 };
+
+// A density on the device as a correlator takes it: FP64 cells, or the FP32
+// cells of an FP32 grid.
+struct Density {
+  const void *p;
+  bool f32;
+};
+inline Density density_of(const Grid *g) { return {g->raw(), g->fp32()}; }
 
 inline Grid *as_grid(fc_grid *g) {
   FC_REQUIRE(g, FC_ERR_INVALID, "null grid handle");
@@ -68,6 +88,10 @@ void device_fill(double *a, size_t n, double v, cudaStream_t s);
 // 2*kSumBlocks + 2 doubles; the results land in scratch[2*kSumBlocks + {0,1}].
 void device_sum_sumsq(const double *a, size_t n, double *scratch,
                       cudaStream_t s);
+void device_sum_sumsq(const float *a, size_t n, double *scratch,
+                      cudaStream_t s);
+// out[i] = (double)in[i].
+void device_widen(const float *in, double *out, size_t n, cudaStream_t s);
 
 // Makes stream `waiter` wait for all work queued so far on `producer`.
 inline void stream_after(cudaStream_t waiter, cudaStream_t producer) {

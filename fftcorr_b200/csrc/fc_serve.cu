@@ -90,7 +90,8 @@ std::string grid_key(const fc_job &j) {
   s.precision(17);
   s << "grid " << j.shape[0] << "x" << j.shape[1] << "x" << j.shape[2] << " "
     << j.cell << " " << j.posmin[0] << "," << j.posmin[1] << "," << j.posmin[2]
-    << " s" << j.scheme << " p" << (j.kind == FC_PERIODIC);
+    << " s" << j.scheme << " p" << (j.kind == FC_PERIODIC) << " f"
+    << j.precision;
   return s.str();
 }
 
@@ -104,8 +105,10 @@ std::string corr_key(const fc_job &j) {
   return s.str();
 }
 
+// A job's grids have the cells of its precision (FP32 for FP32-mixed jobs).
 size_t grid_bytes(const fc_job &j) {
-  return (size_t)j.shape[0] * j.shape[1] * j.shape[2] * sizeof(double) +
+  const size_t cell = j.precision == FC_FP32_MIXED ? sizeof(float) : sizeof(double);
+  return (size_t)j.shape[0] * j.shape[1] * j.shape[2] * cell +
          (2 * kSumBlocks + 2) * sizeof(double);
 }
 
@@ -418,7 +421,7 @@ struct Server {
     // Build what is not resident yet.
     for (Resident *r : grids) {
       if (!r->grid) {
-        r->grid.reset(new Grid(s.shape, s.posmin, s.cell));
+        r->grid.reset(new Grid(s.shape, s.posmin, s.cell, s.precision));
         r->ma = assignor_new(r->grid.get(), s.scheme, s.kind == FC_PERIODIC);
       }
     }

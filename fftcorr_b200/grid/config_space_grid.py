@@ -10,6 +10,12 @@ returns a float64 numpy array that mirrors it: the first access turns the
 mirror on, after which the mirror is refreshed after every device-side change
 and uploaded before every device-side use, so in-place numpy edits such as
 ``dens -= mean`` behave like edits of the reference's aliased view.
+
+Extension beyond the reference: a keyword-only ``precision`` ("fp64", the
+default and the reference's type, or "fp32").  An FP32 grid stores FP32
+cells, which the FP32-mixed correlators read directly; mass assignment still
+sums in FP64 and rounds once per update of a cell, and ``.data`` is still a
+float64 mirror.
 """
 import ctypes
 
@@ -17,10 +23,19 @@ import numpy as np
 
 from fftcorr_b200 import _lib
 
+_CELL_PRECISIONS = {"fp64": _lib.FC_FP64, "fp32": _lib.FC_FP32_MIXED}
+
+
+def _cell_precision(precision):
+    if precision not in _CELL_PRECISIONS:
+        raise ValueError(f"precision must be 'fp64' or 'fp32', got {precision!r}")
+    return _CELL_PRECISIONS[precision]
+
 
 class ConfigSpaceGrid:
     def __init__(self, shape, posmin, posmax, cell_size=None, padding=0,
-                 extra_pad=0, metadata=None):
+                 extra_pad=0, metadata=None, *, precision="fp64"):
+        prec = _cell_precision(precision)
         shape = np.ascontiguousarray(shape, dtype=np.intc)
         posmin = np.asarray(posmin, dtype=np.double).copy(order="C")
         posmax = np.asarray(posmax, dtype=np.double).copy(order="C")
@@ -78,14 +93,17 @@ class ConfigSpaceGrid:
         self._handle = None
         self._host = None
         self._mirror = False
+        self._precision = precision
         h = ctypes.c_void_p()
-        _lib.call("fc_grid_create", _lib.iptr(shape), _lib.dptr(posmin),
-                  self._cell_size, ctypes.byref(h))
+        _lib.call("fc_grid_create_precision", _lib.iptr(shape), _lib.dptr(posmin),
+                  self._cell_size, prec, ctypes.byref(h))
         self._handle = h
 
     @classmethod
-    def from_geometry(cls, shape, posmin, cell_size, metadata=None):
+    def from_geometry(cls, shape, posmin, cell_size, metadata=None, *,
+                      precision="fp64"):
         """A grid with posmin and cell size given directly (no printing)."""
+        prec = _cell_precision(precision)
         self = cls.__new__(cls)
         shape = np.ascontiguousarray(shape, dtype=np.intc)
         posmin = np.asarray(posmin, dtype=np.double).copy(order="C")
@@ -99,9 +117,10 @@ class ConfigSpaceGrid:
         self._metadata = dict(metadata or {})
         self._host = None
         self._mirror = False
+        self._precision = precision
         h = ctypes.c_void_p()
-        _lib.call("fc_grid_create", _lib.iptr(shape), _lib.dptr(posmin),
-                  self._cell_size, ctypes.byref(h))
+        _lib.call("fc_grid_create_precision", _lib.iptr(shape), _lib.dptr(posmin),
+                  self._cell_size, prec, ctypes.byref(h))
         self._handle = h
         return self
 
@@ -130,9 +149,14 @@ class ConfigSpaceGrid:
             _lib.call("fc_grid_download", self._handle, _lib.dptr(self._host))
 
     def device_ptr(self):
+        """Device address of the cells (FP64, or FP32 for an FP32 grid)."""
         p = ctypes.c_void_p()
-        _lib.call("fc_grid_device_ptr", self._handle, ctypes.byref(p))
+        _lib.call("fc_grid_device_data", self._handle, ctypes.byref(p))
         return p.value
+
+    @property
+    def precision(self):
+        return self._precision
 
     # ------------------------------------------------------- properties
     @property

@@ -82,14 +82,27 @@ typedef struct fc_grid fc_grid;
  * memory (config_space_grid.h:12-16). */
 int fc_grid_create(const int shape[3], const double posmin[3],
                    double cell_size, fc_grid **out);
+/* The same grid with a cell type: FC_FP64 (as fc_grid_create) or
+ * FC_FP32_MIXED, FP32 cells for the FP32-mixed correlators, which then read
+ * the grid without a conversion.  Mass assignment into an FP32 grid sums in
+ * FP64 and rounds once per update of a cell; the host copies, sums and
+ * arithmetic below work on either, in FP64 per cell.  (A library extension:
+ * the reference's grids are always FP64.) */
+int fc_grid_create_precision(const int shape[3], const double posmin[3],
+                             double cell_size, int precision, fc_grid **out);
+int fc_grid_precision(const fc_grid *grid, int *precision);
 int fc_grid_destroy(fc_grid *grid);
 /* ConfigSpaceGrid::clear (config_space_grid.h:27). */
 int fc_grid_clear(fc_grid *grid);
-/* Host <-> device copies of the N0*N1*N2 row-major FP64 grid. */
+/* Host <-> device copies of the N0*N1*N2 row-major grid, FP64 on the host
+ * (an FP32 grid rounds each cell once on upload). */
 int fc_grid_upload(fc_grid *grid, const double *host);
 int fc_grid_download(const fc_grid *grid, double *host);
-/* Device pointer of the grid data (valid until fc_grid_destroy). */
+/* Device pointer of an FP64 grid's data (valid until fc_grid_destroy);
+ * FC_ERR_INVALID for an FP32 grid. */
 int fc_grid_device_ptr(const fc_grid *grid, double **device_ptr);
+/* Device pointer of the cells of either precision (fc_grid_precision). */
+int fc_grid_device_data(const fc_grid *grid, void **device_ptr);
 /* ConfigSpaceGrid::get_grid_coords (config_space_grid.h:31-46); *inside is
  * set to 1 or 0 like the reference's bool return. */
 int fc_grid_coords(const fc_grid *grid, const double survey[3], int periodic,
@@ -99,8 +112,9 @@ int fc_grid_sum(fc_grid *grid, double *sum, double *sumsq);
 /* array_ops::add_scalar / multiply_by (array_ops.cc:55-93). */
 int fc_grid_add_scalar(fc_grid *grid, double s);
 int fc_grid_multiply_by(fc_grid *grid, double s);
-/* y += a * x elementwise (same shapes).  Used to form N = D - alpha R from
- * separately assigned catalogs. */
+/* y += a * x elementwise (same shapes; precisions may differ, each cell
+ * computed in FP64).  Used to form N = D - alpha R from separately
+ * assigned catalogs. */
 int fc_grid_axpy(fc_grid *y, double a, const fc_grid *x);
 
 /* ---------------------------------------------------------- MassAssignor */
@@ -295,8 +309,9 @@ int fc_apply_displacement(const fc_grid *grid, const double *pos, int64_t n,
  * CLI (cc/fftcorr.cc:233-463): periodic: assign, delta = (rho - mean)/mean,
  * autocorrelate; survey: NN = D - alpha R (alpha = sum w_D / sum w_R, the
  * randoms negated as fftcorr/fftcorr.py:538 does), autocorrelate, and with
- * want_rr also the RR grid.  Results equal a job run alone.  Has no
- * counterpart in the reference. */
+ * want_rr also the RR grid.  The grids have the job's precision: FP32 cells
+ * for FP32-mixed jobs (fc_grid_create_precision).  Results equal a job run
+ * alone.  Has no counterpart in the reference. */
 typedef struct fc_job {
   int kind;                 /* FC_PERIODIC or FC_SURVEY                    */
   int shape[3];

@@ -97,7 +97,8 @@ def test_periodic_job_equals_direct_api():
     t = srv.submit(spec)
     got = _collect(srv, [t], [spec])[0][0]
     srv.close()
-    g = fb.ConfigSpaceGrid.from_geometry((n, n, n), [0, 0, 0], L / n)
+    # A served FP32-mixed job works on FP32 grids.
+    g = fb.ConfigSpaceGrid.from_geometry((n, n, n), [0, 0, 0], L / n, precision="fp32")
     ma = fb.MassAssignor(g, fb.DistributionScheme.CLOUD_IN_CELL, True, 0)
     ma.add_particles(posw)
     mean = ma.totw / n ** 3
@@ -124,8 +125,8 @@ def test_survey_job_equals_direct_api():
     R = catalog.DeviceCatalog(j.randoms.n)
     _lib.call("fc_catalog_generate", j.randoms, ctypes.c_void_p(R.ptr))
     shape, posmin, cell = tuple(j.shape), tuple(j.posmin), j.cell
-    gA = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell)
-    gB = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell)
+    gA = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell, precision="fp32")
+    gB = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell, precision="fp32")
     tsc = fb.DistributionScheme.TRIANGULAR_SHAPED_CLOUD
     mA = fb.MassAssignor(gA, tsc, False, 0)
     mB = fb.MassAssignor(gB, tsc, False, 0)
