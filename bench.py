@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--mix-jobs", type=int, default=48)
     ap.add_argument("--mix-rate", type=float, default=6.0)
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
+    # Wraps the FP32 form's timed steps in fc_profiler_range, for a launch
+    # list taken with `ncu --profile-from-start off`.
+    ap.add_argument("--profile-range", action="store_true")
     return ap.parse_args()
 
 
@@ -740,15 +743,19 @@ def main():
     dD, dR = device_copy(D), device_copy(R)
     timer = DeviceTimer()
 
-    def timed(fn, steps, warmup):
+    def timed(fn, steps, warmup, profile=False):
         for _ in range(warmup):
             fn()
         dist.barrier()
         n0 = _lib.launch_count()
+        if profile:
+            _lib.call("fc_profiler_range", 1)
         timer.start()
         for _ in range(steps):
             out = fn()
         secs = timer.stop()
+        if profile:
+            _lib.call("fc_profiler_range", 0)
         timed.launches = _lib.launch_count() - n0
         return dist.max(secs), out
 
@@ -756,7 +763,7 @@ def main():
     job = SurveyJob(w, "fp32")
     with ClockSampler(local) as clocks:
         t_dev, (nn, rr, xi) = timed(lambda: job.run_device(dD, nD, dR, nR),
-                                    a.steps, a.warmup)
+                                    a.steps, a.warmup, a.profile_range)
     launches_dev = timed.launches
     rs, ks = subgrid_dims(job.corr)
     t_e2e_sync, _ = timed(lambda: job.run_host(D, R), a.steps, 1)

@@ -132,6 +132,7 @@ _SIGNATURES = {
     "fc_last_error": (ctypes.c_char_p, []),
     "fc_version": (ctypes.c_int, []),
     "fc_launch_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
+    "fc_profiler_range": (ctypes.c_int, [ctypes.c_int]),
     "fc_set_device": (ctypes.c_int, [ctypes.c_int]),
     "fc_grid_create": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_double, c_void_pp]),
     "fc_grid_create_precision": (ctypes.c_int, [c_int_p, c_double_p, ctypes.c_double,

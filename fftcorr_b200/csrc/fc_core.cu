@@ -8,6 +8,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda_profiler_api.h>
+
 #include "fc_common.cuh"
 #include "fc_internal.h"
 
@@ -259,6 +261,15 @@ int fc_launch_count(unsigned long long *count) {
   return guard([&] {
     FC_REQUIRE(count, FC_ERR_INVALID, "null argument");
     *count = fc::launch_counter().load(std::memory_order_relaxed);
+  });
+}
+
+int fc_profiler_range(int on) {
+  return guard([&] {
+    if (on)
+      FC_CUDA(cudaProfilerStart());
+    else
+      FC_CUDA(cudaProfilerStop());
   });
 }
 

@@ -482,6 +482,11 @@ int fc_sum_sumsq_static(const double *device_data, int64_t n, double *sum,
 int fc_launch_count(unsigned long long *count);
 /* Waits for all work on the current device. */
 int fc_device_synchronize(void);
+/* Marks the start (on != 0) or end of a region for a profiler started with
+ * capture off until the region (cudaProfilerStart / cudaProfilerStop), so a
+ * launch list can cover one timed step of a longer run.  Has no counterpart
+ * in the reference. */
+int fc_profiler_range(int on);
 /* Page-locks an existing host range so copies from it run at full PCIe
  * speed (cudaHostRegister), and releases it. */
 int fc_host_register(void *ptr, size_t bytes);
