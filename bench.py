@@ -308,8 +308,8 @@ def kernel_profile(job, dD, nD, dR, nR):
 TRAFFIC_PER_LAUNCH_512 = {
     "zfwd": 1048.8e6,
     "yfwd": 1063.2e6,
-    "xcorr": 1372.2e6,
-    "xcorr00": 792.8e6,
+    "xcorr": 1375.7e6,
+    "xcorr00": 801.0e6,
     "yinv": 144.4e6,
     "zinv": 49.1e6,
 }

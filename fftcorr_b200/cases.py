@@ -12,7 +12,8 @@ grid of the same precision (FP32 cells for fp32), once to warm up and then
 (ell <= 2) on a seeded random grid, FP32 then FP64, two runs each.  batch:
 six periodic boxes (128^3, 192^3, 256^3; 1M clustered particles each) in one
 CUDA graph, run twice.  assign: TSC mass assignment of seeded uniform
-sector randoms onto the benchmark's 512^3 grid.
+sector randoms onto the benchmark's 512^3 grid (FP32 cells for fp32, the
+FP32-mixed form's grids).
 
 Each case holds a few GB of device memory at most, with inputs larger than
 the 126 MB L2, so per-kernel DRAM figures are meaningful.  Everything goes
@@ -74,7 +75,7 @@ def _assign(a):
     shape = (512,) * 3
     posmin, cell = mocks.survey_box(sector, 200.0, shape)
     R = mocks.sector_randoms(int(a.n), 3, sector=sector)
-    grid = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell)
+    grid = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell, precision=a.precision)
     ma = fb.MassAssignor(grid, fb.DistributionScheme.TRIANGULAR_SHAPED_CLOUD, False, 0)
     ma.add_particles(R)
 
