@@ -579,6 +579,14 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
       // Each thread stages up to kSlots particles: the index loads first,
       // then the catalog rows as asynchronous copies, so the gathers of one
       // thread overlap.
+      // The keys this thread's warp ranks below are read here, together
+      // with the indices, so that both loads are in flight at once.
+      KeyT kr[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = warp * 32 * R + r * 32 + lane;
+        kr[r] = i < m ? keys[c0 + i] : kbase + (KeyT)T;
+      }
       uint32_t idx[kSlots];
 #pragma unroll
       for (int j = 0; j < kSlots; ++j) {
@@ -611,7 +619,7 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
         const int i = warp * 32 * R + r * 32 + lane;
         // (A key outside this unit cannot occur in a correct sort; it is
         // dropped rather than indexing outside the unit's cells.)
-        const KeyT kd = i < m ? keys[c0 + i] - kbase : (KeyT)T;
+        const KeyT kd = kr[r] - kbase;
         const int cell = kd < (KeyT)T ? (int)kd : -1;
         const unsigned peers = __match_any_sync(0xffffffffu, cell);
         const int leader = __ffs(peers) - 1;
