@@ -36,8 +36,8 @@ namespace {
 // add_scalar(-mean) then multiply_by(1/mean) (fftcorr.cc:369-375), written
 // straight into the padded work grid in the transform precision.  mean =
 // totw / ncells from the assignor's device totals.
-template <typename T>
-__global__ void k_norm_pad(const double *__restrict__ rho, T *__restrict__ work,
+template <typename TI, typename T>
+__global__ void k_norm_pad(const TI *__restrict__ rho, T *__restrict__ work,
                            int n0, int n1, int n2, int n2p,
                            const double *__restrict__ totals, double ncells) {
   const double mean = totals[0] / ncells;
@@ -45,10 +45,12 @@ __global__ void k_norm_pad(const double *__restrict__ rho, T *__restrict__ work,
   const double scale = 1.0 / mean;
   const size_t nrows = (size_t)n0 * n1;
   for (size_t row = blockIdx.x; row < nrows; row += gridDim.x) {
-    const double *src = rho + row * n2;
+    const TI *src = rho + row * n2;
     T *dst = work + row * n2p;
+    // Rounded to the cell type after each step, as fc_grid_add_scalar and
+    // fc_grid_multiply_by round a grid's cells (a no-op for FP64 cells).
     for (int k = threadIdx.x; k < n2; k += blockDim.x)
-      dst[k] = (T)((src[k] + shift) * scale);
+      dst[k] = (T)((double)(TI)((double)src[k] + shift) * scale);
   }
 }
 
@@ -207,7 +209,8 @@ struct Batch {
     FC_CUDA(cudaEventCreate(&t1));
     const double zero[3] = {0, 0, 0};
     for (auto &b : boxes) {
-      grids.emplace_back(new Grid(b.shape, zero, b.cell));
+      // Grids of the batch's precision: FP32 cells in the FP32-mixed form.
+      grids.emplace_back(new Grid(b.shape, zero, b.cell, prm.precision));
       Grid *g = grids.back().get();
       mas.push_back(assignor_new(g, prm.scheme, true));
       assignor_prepare_graph(mas.back(), b.n, g->stream);
@@ -259,16 +262,22 @@ struct Batch {
     const LaunchShape &ls = ls_norm[i];
     const unsigned blocks =
         (unsigned)std::min<size_t>(nrows, (size_t)sm_count() * ls.waves);
-    k_norm_pad<T><<<blocks, ls.threads, 0, s>>>(
-        grids[i]->ptr(), static_cast<T *>(correlator_work(corrs[i])), b.shape[0],
-        b.shape[1], b.shape[2], n2p, assignor_totals(mas[i]),
-        (double)grids[i]->size());
+    T *work = static_cast<T *>(correlator_work(corrs[i]));
+    const Grid *g = grids[i].get();
+    if (g->fp32())
+      k_norm_pad<float, T><<<blocks, ls.threads, 0, s>>>(
+          static_cast<const float *>(g->raw()), work, b.shape[0], b.shape[1],
+          b.shape[2], n2p, assignor_totals(mas[i]), (double)g->size());
+    else
+      k_norm_pad<double, T><<<blocks, ls.threads, 0, s>>>(
+          g->ptr(), work, b.shape[0], b.shape[1], b.shape[2], n2p,
+          assignor_totals(mas[i]), (double)g->size());
     FC_LAUNCH_CHECK();
   }
 
   void enqueue_box(int i, cudaStream_t s) {
     Grid *g = grids[i].get();
-    FC_CUDA(cudaMemsetAsync(g->ptr(), 0, g->size() * sizeof(double), s));
+    FC_CUDA(cudaMemsetAsync(g->raw(), 0, g->size() * g->cell_bytes(), s));
     assignor_enqueue_graph(mas[i], boxes[i].posw, boxes[i].n, s);
     if (fp64())
       norm_pad<double>(i, s);

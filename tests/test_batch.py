@@ -40,7 +40,8 @@ def _boxes():
 
 
 def _single_box(shape, cell, posw, precision, maxell=2):
-    g = fb.ConfigSpaceGrid.from_geometry(shape, [0, 0, 0], cell)
+    # The batch's grids have its precision (FP32 cells in the FP32 form).
+    g = fb.ConfigSpaceGrid.from_geometry(shape, [0, 0, 0], cell, precision=precision)
     ma = fb.MassAssignor(g, fb.DistributionScheme.CLOUD_IN_CELL, True, 0)
     ma.add_particles(np.ascontiguousarray(posw))
     mean = ma.totw / (shape[0] * shape[1] * shape[2])
