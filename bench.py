@@ -329,6 +329,8 @@ def algorithmic_bytes(family, w, precision, rs, ks):
     each result written once).  Survey fused passes, N = N0 N1 N2 cells,
     h = N2/2 + 1, Nc = N0 N1 h complex cells of e bytes (8 FP32, 16 FP64):
       zfwd   density in (N * s) + W out (Nc * e)
+      zfwd2  the z pass of two terms at once: density in (N * s) + two W
+             out (2 Nc e)
       yfwd   W in and out (2 Nc e)
       xcorr  W and G in (2 Nc e) + x-pruned Wr out (rs N1 h e)
              + k-subgrid weight read (s bytes a cell) and FP64
@@ -347,6 +349,7 @@ def algorithmic_bytes(family, w, precision, rs, ks):
     kc = ks[0] * ks[1] * ks[2]
     table = {
         "zfwd": n * s + nc * e,
+        "zfwd2": n * s + 2 * nc * e,
         "yfwd": 2 * nc * e,
         "xcorr": 2 * nc * e + rs * n1 * h * e + kc * (16 + s),
         "xcorr00": nc * e + rs * n1 * h * e + kc * (16 + s),

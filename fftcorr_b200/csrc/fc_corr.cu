@@ -23,6 +23,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -898,18 +899,39 @@ struct Correlator {
       const void *in = prepared ? fused->input(d.p, d.f32)
                                 : fused->prepare_input(d.p, d.f32, stream);
       ProfHook hook(&prof, stream);
+      PhaseHook *ph = prof.on ? &hook : nullptr;
       const KAxes ka = kaxes();
+      // This correlator's terms in order.  Consecutive weighted terms
+      // (ell > 0) share one z pass where the passes allow it; the second
+      // term's z result waits in the fused passes' second buffer.
+      std::vector<std::array<int, 2>> owned;
       int term = 0;
+      for (int ell = 0; ell <= maxell; ell += 2)
+        for (int m = -ell; m <= ell; ++m)
+          if (owns_term(term++)) owned.push_back({ell, m});
+      size_t next = 0;
+      bool second_ready = false;
       for (int ell = 0; ell <= maxell; ell += 2) {
         zero_sub(true, true);
-        for (int m = -ell; m <= ell; ++m) {
-          if (!owns_term(term++)) continue;
+        for (; next < owned.size() && owned[next][0] == ell; ++next) {
+          const int m = owned[next][1];
+          bool z_done = false;
+          if (second_ready) {
+            fused->take_second();
+            z_done = true;
+            second_ready = false;
+          } else if (ell > 0 && next + 1 < owned.size() && fused->pairs()) {
+            fused->zfwd_pair(in, ell, m, owned[next + 1][0], owned[next + 1][1],
+                             xyz0, stream, ph);
+            z_done = true;
+            second_ready = true;
+          }
           // One forward and one (pruned) inverse transform, or the inverse
           // alone for the ell = 0 term of an autocorrelation.
           n_fft += fused->term(in, ell, m, xyz0, (double)ncells,
                                ksub.as<double>(), rsub.as<double>(),
-                               d_raxis.as<double>(), ka, stream,
-                               prof.on ? &hook : nullptr, prepared);
+                               d_raxis.as<double>(), ka, stream, ph, prepared,
+                               z_done);
         }
         hist_rows(ell, true, true);
         if (ell == 0) save_zerolag();
@@ -1093,8 +1115,12 @@ size_t correlator_footprint(int kind, const int shape[3], double cell,
     bytes += 2 * (size_t)g.shape[0] * g.shape[1] * h * eb;   // W, G
     bytes += (size_t)g.rsize * g.shape[1] * h * eb;          // Wr
     bytes += (size_t)g.rsize * g.rsize * h * eb;             // Wry
-    if (precision != FC_FP64)                                // FP32 density,
+    if (precision != FC_FP64) {                              // FP32 density,
       bytes += g.ncells() * 4 + (size_t)g.shape[0] * g.shape[1] * 32;  // row table
+      const int m = g.shape[2] / 2;
+      if (m >= 64 && m <= 2048 && (m & (m - 1)) == 0)        // paired z pass:
+        bytes += (size_t)g.shape[0] * g.shape[1] * (h * eb + 32);  // W2, table
+    }
     const int nlm = maxell == 0 ? 1 : maxell == 2 ? 6 : 15;
     bytes += (size_t)nlm * g.kcells() * rb;                  // k weights
     bytes += (size_t)nlm * g.rsize * g.rsize * g.rsize * rb; // r weights

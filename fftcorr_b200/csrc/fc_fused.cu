@@ -1214,6 +1214,111 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   }
 }
 
+// Weighting of one row's eight pairs of cells for an (ell > 0, m) term, out
+// = Y_lm * in (out may be in), in the form row_poly_form picks (one
+// uniform branch per thread, as in k_zfwd_pp).
+template <int TPC>
+__device__ __forceinline__ void weigh_row(const RowPoly &rp, const YlmParams &p,
+                                          float zt, const float2 *in,
+                                          float2 *out) {
+  auto weigh = [&](auto poly, auto ellc) {
+    constexpr int POLY = decltype(poly)::value, ELL = decltype(ellc)::value;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const float zu = zt + (float)(2 * TPC * u);
+      const float2 c = in[u];
+      out[u].x = row_weight_form<POLY, ELL>(rp, c.x, zu);
+      out[u].y = row_weight_form<POLY, ELL>(rp, c.y, zu + 1.0f);
+    }
+  };
+  using std::integral_constant;
+  using I2 = integral_constant<int, 2>;
+  using I4 = integral_constant<int, 4>;
+  if (p.ell == 2) {
+    switch (row_poly_form(2, p.m)) {
+      case 0: weigh(integral_constant<int, 0>(), I2()); break;
+      case 1: weigh(integral_constant<int, 1>(), I2()); break;
+      default: weigh(integral_constant<int, 2>(), I2()); break;
+    }
+  } else {
+    switch (row_poly_form(4, p.m)) {
+      case 0: weigh(integral_constant<int, 0>(), I4()); break;
+      case 1: weigh(integral_constant<int, 1>(), I4()); break;
+      case 2: weigh(integral_constant<int, 2>(), I4()); break;
+      case 3: weigh(integral_constant<int, 3>(), I4()); break;
+      default: weigh(integral_constant<int, 4>(), I4()); break;
+    }
+  }
+}
+
+// The weighted z pass of two (ell > 0, m) terms at once: thread t of row
+// group pb holds z[t + TPC u] of one row, and its two transforms are that
+// row weighted for term a and for term b.  The density row is read once
+// for both terms and each term's W gets its row, so a pair of terms reads
+// the density once instead of twice; the transform and the real-to-complex
+// split are those of k_zfwd_pp.
+template <int L>
+__global__ void __launch_bounds__(PP<L>::THREADS)
+    k_zfwd_pp2(const float *__restrict__ rho, float2 *__restrict__ Wa,
+               float2 *__restrict__ Wb, FusedGeom g, YlmParams pa, YlmParams pq,
+               double z0, const float2 *__restrict__ tabz,
+               const float4 *__restrict__ rowtab_a,
+               const float4 *__restrict__ rowtab_b) {
+  using Q = PP<L>;
+  constexpr int RP = L + L / 8 + 1;
+  extern __shared__ unsigned char smem_raw[];
+  CPairS *ex = reinterpret_cast<CPairS *>(smem_raw);
+  const int pb = threadIdx.x / Q::TPC;
+  const int t = threadIdx.x - pb * Q::TPC;
+  const int64_t nrows = (int64_t)g.n0 * g.n1;
+  const int64_t row = (int64_t)blockIdx.x * Q::PB + pb;
+  const bool valid = row < nrows;
+  const int64_t r = valid ? row : 0;
+  const float2 *src = reinterpret_cast<const float2 *>(rho + r * g.n2);
+  const RowPoly ra = load_row_poly(rowtab_a, r, pa);
+  const RowPoly rq = load_row_poly(rowtab_b, r, pq);
+  const float zt = (float)(z0 + (2 * t) * 1.0);
+  const float2 zero = make_float2(0.f, 0.f);
+  float2 a[8], b[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) a[u] = valid ? src[t + Q::TPC * u] : zero;
+  weigh_row<Q::TPC>(rq, pq, zt, a, b);
+  weigh_row<Q::TPC>(ra, pa, zt, a, a);
+  CPairS v[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) v[u] = cpack_s(a[u], b[u]);
+  auto exf = [&](int i) { return &ex[pb * RP + i + (i >> 3)]; };
+  reg_fft<L>(v, t, exf, tabz, -1, 2);
+#pragma unroll
+  for (int u = 0; u < 8; ++u) *exf(t + Q::TPC * u) = v[u];
+  __syncthreads();
+  if (!valid) return;
+  float2 *dst0 = Wa + row * g.hp;
+  float2 *dst1 = Wb + row * g.hp;
+#pragma unroll
+  for (int i = 0; i <= L / 2 / Q::TPC; ++i) {
+    const int k = t + Q::TPC * i;
+    if (k > L / 2) break;
+    const CPairS za = *exf(k);
+    const CPairS c = cconj(*exf(k == 0 ? 0 : L - k));
+    CPairS e, o;
+    e.x = 0.5f * (za.x + c.x);
+    e.y = 0.5f * (za.y + c.y);
+    const CPairS d = csub(za, c);
+    o.x = 0.5f * d.y;
+    o.y = -0.5f * d.x;
+    const CPairS ow = cmul(o, __ldg(&tabz[k]));
+    const CPairS rr = cadd(e, ow);
+    dst0[k] = clane0(rr);
+    dst1[k] = clane1(rr);
+    if (k != L / 2) {
+      const CPairS q = cconj(csub(e, ow));
+      dst0[L - k] = clane0(q);
+      dst1[L - k] = clane1(q);
+    }
+  }
+}
+
 // Per-row Horner coefficients of one (ell, m) (row_poly), two float4 per
 // row, so the z pass does no FP64 work per row.
 __global__ void k_rowpoly(float4 *__restrict__ tab, int64_t nrows, int n1,
@@ -1379,6 +1484,8 @@ void p2_set_limits() {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
     FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp<L, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+    FC_CUDA(cudaFuncSetAttribute(k_zfwd_pp2<L>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   }
 }
 
@@ -1434,6 +1541,10 @@ FusedSurvey::FusedSurvey(const int shape[3], int rsize, const int kshape[3],
   if (!fp64) {
     rho32.resize((size_t)g.n0 * g.n1 * g.n2 * sizeof(float));
     rowtab.resize((size_t)g.n0 * g.n1 * 2 * sizeof(float4));
+    if (pairs()) {
+      W2.resize(nc * eb);
+      rowtab2.resize((size_t)g.n0 * g.n1 * 2 * sizeof(float4));
+    }
   }
   set_smem_limits();
 }
@@ -1763,10 +1874,39 @@ void FusedSurvey::grid2(const void *rho_in, cudaStream_t s, const KAxes &ka) {
   }
 }
 
+bool FusedSurvey::pairs() const { return !fp64_ && is_p2(g.m); }
+
+void FusedSurvey::zfwd_pair(const void *rho_in, int ell_a, int m_a, int ell_b,
+                            int m_b, const double xyz0[3], cudaStream_t s,
+                            PhaseHook *hook) {
+  FC_REQUIRE(pairs() && ell_a > 0 && ell_b > 0, FC_ERR_STATE,
+             "paired z pass needs two weighted FP32 terms");
+  const YlmParams pa = make_ylm_params(ell_a, m_a, 1.0);
+  const YlmParams pb = make_ylm_params(ell_b, m_b, 1.0);
+  const int64_t nrows = (int64_t)g.n0 * g.n1;
+  k_rowpoly<<<grid_for(nrows, 256), 256, 0, s>>>(rowtab.as<float4>(), nrows,
+                                                 g.n1, pa, xyz0[0], xyz0[1]);
+  FC_LAUNCH_CHECK();
+  k_rowpoly<<<grid_for(nrows, 256), 256, 0, s>>>(rowtab2.as<float4>(), nrows,
+                                                 g.n1, pb, xyz0[0], xyz0[1]);
+  FC_LAUNCH_CHECK();
+  if (hook) hook->begin("zfwd2");
+  with_p2(g.m, [&]<int L>() {
+    using PQ = PP<L>;
+    const unsigned blocks = (unsigned)((nrows + PQ::PB - 1) / PQ::PB);
+    k_zfwd_pp2<L><<<blocks, PQ::THREADS, p2_row_smem<float, L>(), s>>>(
+        static_cast<const float *>(rho_in), W.as<float2>(), W2.as<float2>(), g,
+        pa, pb, xyz0[2], tabz.as<float2>(), rowtab.as<float4>(),
+        rowtab2.as<float4>());
+  });
+  FC_LAUNCH_CHECK();
+  if (hook) hook->end();
+}
+
 int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
                        double ncells, double *ksub, double *rsub,
                        const double *raxis, const KAxes &ka, cudaStream_t s,
-                       PhaseHook *hook, bool g_of_input) {
+                       PhaseHook *hook, bool g_of_input, bool z_done) {
   const YlmParams pw = make_ylm_params(ell, m, 1.0);
   const YlmParams pr = make_ylm_params(ell, m, 4.0 * M_PI / ncells);
   const void *ktab = ksub ? k_table(ell, m, ka, s) : nullptr;
@@ -1781,9 +1921,11 @@ int FusedSurvey::term(const void *rho_in, int ell, int m, const double xyz0[3],
       xcorr00<T>(ksub, ktab, pw.value0, s);
       if (hook) hook->end();
     } else {
-      if (hook) hook->begin("zfwd");
-      zfwd<T>(rho_in, true, pw, xyz0, s);
-      if (hook) hook->end();
+      if (!z_done) {
+        if (hook) hook->begin("zfwd");
+        zfwd<T>(rho_in, true, pw, xyz0, s);
+        if (hook) hook->end();
+      }
       if (hook) hook->begin("yfwd");
       yfwd<T>(s);
       if (hook) hook->end();

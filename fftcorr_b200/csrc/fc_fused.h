@@ -3,6 +3,7 @@
 #pragma once
 
 #include <map>
+#include <utility>
 #include <vector>
 
 #include "fc_common.cuh"
@@ -63,7 +64,15 @@ class FusedSurvey {
   int term(const void *rho_in, int ell, int m, const double xyz0[3],
             double ncells, double *ksub, double *rsub, const double *raxis,
             const KAxes &ka, cudaStream_t s, PhaseHook *hook,
-            bool g_of_input = false);
+            bool g_of_input = false, bool z_done = false);
+  // Whether two weighted terms can share one z pass (FP32, power-of-two
+  // rows).  zfwd_pair runs the z pass of terms a and b (both ell > 0) in
+  // one launch: term a's result lands in W, term b's in a second buffer
+  // that take_second() swaps into W before term b runs with z_done.
+  bool pairs() const;
+  void zfwd_pair(const void *rho_in, int ell_a, int m_a, int ell_b, int m_b,
+                 const double xyz0[3], cudaStream_t s, PhaseHook *hook);
+  void take_second() { std::swap(W, W2); }
 
   // G in the half-complex layout [N0][N1][N2/2+1] with rows g.hp elements
   // apart (FP64 or FP32 complex).
@@ -101,6 +110,7 @@ class FusedSurvey {
   bool fp64_;
   DeviceBuffer tabx, taby, tabz;
   DeviceBuffer W, G, Wr, Wry, rho32;
+  DeviceBuffer W2, rowtab2;  // the second term of a paired z pass
   std::map<int, DeviceBuffer> ktabs;
   std::map<int, DeviceBuffer> rtabs;
   DeviceBuffer rowtab;  // per-row z-pass weight coefficients (FP32 form)
