@@ -919,6 +919,73 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
 // holds one pair of columns at a time and two CTAs fit an SM; the other
 // CTA's warps cover those loads.
 constexpr int kXB = 16;  // columns per CTA of the FP32 x passes
+
+// k-subgrid extraction of k_xcorr_pp (as in k_xcorr_p2) for the columns c0
+// and c0 + 1 of thread (t, p), from P staged in the exchange slots.  Not
+// inlined, so that its registers do not weigh on the kernel's transforms;
+// only the CTAs whose y and kz reach the k-subgrid call it.
+template <int L>
+__device__ __noinline__ void xcorr_pp_extract(const CPair *ex, int t, int p,
+                                              int c0, int jr0, int jr1, int ks0,
+                                              int ks1, int ks2, int n1,
+                                              double *__restrict__ ksub,
+                                              const float *__restrict__ ktab) {
+  using Q = PY<L, kXB>;
+  const int ox = ks0 / 2, oz = ks2 / 2;
+  auto exf = [&](int i) { return &ex[Q::row(i) * Q::PB + p]; };
+  if (ks0 <= 3 * Q::TPC && ks1 <= n1) {
+    // At most three x rows per thread and one row j per reflection: each
+    // reflection's loads are issued together.
+#pragma unroll
+    for (int refl = 0; refl < 2; ++refl) {
+      const int j = refl == 0 ? jr0 : jr1;
+      if (j >= ks1) continue;
+      size_t cell[3][2];
+      double acc[3][2], w[3][2], re[3][2];
+      bool on[3][2];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int i = t + s * Q::TPC;
+        const int x = refl == 0 ? (i - ox) & (L - 1) : (ox - i) & (L - 1);
+#pragma unroll
+        for (int ln = 0; ln < 2; ++ln) {
+          const int kzi = c0 + ln;
+          on[s][ln] = i < ks0 && kzi <= oz && !(refl == 1 && kzi == 0);
+          const int k = refl == 0 ? kzi + oz : oz - kzi;
+          cell[s][ln] = ((size_t)i * ks1 + j) * ks2 + k;
+          if (on[s][ln]) {
+            re[s][ln] = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
+            w[s][ln] = (double)ktab[cell[s][ln]];
+            acc[s][ln] = ksub[cell[s][ln]];
+          }
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+#pragma unroll
+        for (int ln = 0; ln < 2; ++ln)
+          if (on[s][ln]) ksub[cell[s][ln]] = acc[s][ln] + w[s][ln] * re[s][ln];
+    }
+    return;
+  }
+  for (int ln = 0; ln < 2; ++ln) {
+    const int kzi = c0 + ln;
+    if (kzi > oz) continue;
+    for (int refl = 0; refl < 2; ++refl) {
+      if (refl == 1 && kzi == 0) continue;
+      const int k = refl == 0 ? kzi + oz : oz - kzi;
+      for (int j = refl == 0 ? jr0 : jr1; j < ks1; j += n1) {
+        for (int i = t; i < ks0; i += Q::TPC) {
+          const int x = refl == 0 ? (i - ox) & (L - 1) : (ox - i) & (L - 1);
+          const double re = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
+          const size_t cell = ((size_t)i * ks1 + j) * ks2 + k;
+          ksub[cell] += (double)ktab[cell] * re;
+        }
+      }
+    }
+  }
+}
+
 template <int L, int MODE>
 __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREADS)
     k_xcorr_pp(const float2 *__restrict__ W, const float2 *__restrict__ G,
@@ -967,7 +1034,7 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
       v[u] = cmulc(v[u], load_pair(reinterpret_cast<const float2 *>(exr(u))));
   }
   // k-subgrid extraction, as in k_xcorr_p2, for both columns of the pair.
-  const int ox = g.ks0 / 2, oy = g.ks1 / 2, oz = g.ks2 / 2;
+  const int oy = g.ks1 / 2, oz = g.ks2 / 2;
   const int jr0 = (yy + oy) % g.n1;
   const int jr1 = ((oy - yy) % g.n1 + g.n1) % g.n1;
   if (ksub != nullptr && cb <= oz && (jr0 < g.ks1 || jr1 < g.ks1)) {
@@ -976,58 +1043,9 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
 #pragma unroll
     for (int u = 0; u < 8; ++u) *exr(u) = v[u];
     __syncthreads();
-    if (c0 <= oz) {
-      if (g.ks0 <= 3 * Q::TPC && g.ks1 <= g.n1) {
-#pragma unroll
-        for (int refl = 0; refl < 2; ++refl) {
-          const int j = refl == 0 ? jr0 : jr1;
-          if (j >= g.ks1) continue;
-          size_t cell[3][2];
-          double acc[3][2], w[3][2], re[3][2];
-          bool on[3][2];
-#pragma unroll
-          for (int s = 0; s < 3; ++s) {
-            const int i = t + s * Q::TPC;
-            const int x = refl == 0 ? (i - ox) & (L - 1) : (ox - i) & (L - 1);
-#pragma unroll
-            for (int ln = 0; ln < 2; ++ln) {
-              const int kzi = c0 + ln;
-              on[s][ln] = i < g.ks0 && kzi <= oz && !(refl == 1 && kzi == 0);
-              const int k = refl == 0 ? kzi + oz : oz - kzi;
-              cell[s][ln] = ((size_t)i * g.ks1 + j) * g.ks2 + k;
-              if (on[s][ln]) {
-                re[s][ln] = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
-                w[s][ln] = (double)ktab[cell[s][ln]];
-                acc[s][ln] = ksub[cell[s][ln]];
-              }
-            }
-          }
-#pragma unroll
-          for (int s = 0; s < 3; ++s)
-#pragma unroll
-            for (int ln = 0; ln < 2; ++ln)
-              if (on[s][ln]) ksub[cell[s][ln]] = acc[s][ln] + w[s][ln] * re[s][ln];
-        }
-      } else {
-        for (int ln = 0; ln < 2; ++ln) {
-          const int kzi = c0 + ln;
-          if (kzi > oz) continue;
-          for (int refl = 0; refl < 2; ++refl) {
-            if (refl == 1 && kzi == 0) continue;
-            const int k = refl == 0 ? kzi + oz : oz - kzi;
-            for (int j = refl == 0 ? jr0 : jr1; j < g.ks1; j += g.n1) {
-              for (int i = t; i < g.ks0; i += Q::TPC) {
-                const int x = refl == 0 ? (i - ox) & (L - 1)
-                                        : (ox - i) & (L - 1);
-                const double re = (double)(ln ? exf(x)->x.y : exf(x)->x.x);
-                const size_t cell = ((size_t)i * g.ks1 + j) * g.ks2 + k;
-                ksub[cell] += (double)ktab[cell] * re;
-              }
-            }
-          }
-        }
-      }
-    }
+    if (c0 <= oz)
+      xcorr_pp_extract<L>(ex, t, p, c0, jr0, jr1, g.ks0, g.ks1, g.ks2, g.n1,
+                          ksub, ktab);
 #pragma unroll
     for (int u = 0; u < 8; ++u) v[u] = *exr(u);
     __syncthreads();
