@@ -116,12 +116,16 @@ int64_t max_particles(const fc_job &j) {
   return std::max(j.data.n, j.kind == FC_SURVEY ? j.randoms.n : (int64_t)0);
 }
 
-// Device bytes of a worker's catalog staging for job j: the largest catalog
-// plus scratch for its cluster centres.
+size_t stage_rows_bytes(int64_t n) { return ((size_t)n * 32 + 255) / 256 * 256; }
+
+// Device bytes of a worker's catalog staging for job j: every catalog of
+// the job (a survey's data and randoms side by side, so the randoms can be
+// copied in while the data are assigned) plus scratch for cluster centres.
 size_t job_stage_bytes(const fc_job &j) {
   const size_t cs = std::max(catalog_scratch_bytes(j.data),
                              j.kind == FC_SURVEY ? catalog_scratch_bytes(j.randoms) : 0);
-  return ((size_t)max_particles(j) * 32 + 255) / 256 * 256 + cs;
+  return stage_rows_bytes(j.data.n) +
+         (j.kind == FC_SURVEY ? stage_rows_bytes(j.randoms.n) : 0) + cs;
 }
 
 void validate(const fc_job &j) {
@@ -176,17 +180,41 @@ struct Server {
   // bytes_resident).
   std::vector<std::unique_ptr<DeviceBuffer>> stage;
   std::vector<size_t> stage_bytes;
+  // Per-worker stream for catalog copies (or generation) and the events
+  // that mark each catalog in.
+  std::vector<cudaStream_t> copy_stream;
+  std::vector<cudaEvent_t> data_in, randoms_in;
 
   Server(size_t budget_, int slots_, int max_bypass_)
       : budget(budget_), slots(slots_), max_bypass(max_bypass_) {
     FC_REQUIRE(slots >= 1 && slots <= 64, FC_ERR_INVALID, "slots must be 1..64");
     FC_REQUIRE(budget > 0, FC_ERR_INVALID, "budget must be positive");
     FC_CUDA(cudaGetDevice(&device));
-    for (int i = 0; i < slots; ++i) {
-      stage.emplace_back(new DeviceBuffer);
-      stage_bytes.push_back(0);
+    copy_stream.assign(slots, nullptr);
+    data_in.assign(slots, nullptr);
+    randoms_in.assign(slots, nullptr);
+    try {
+      for (int i = 0; i < slots; ++i) {
+        stage.emplace_back(new DeviceBuffer);
+        stage_bytes.push_back(0);
+        FC_CUDA(cudaStreamCreateWithFlags(&copy_stream[i], cudaStreamNonBlocking));
+        FC_CUDA(cudaEventCreateWithFlags(&data_in[i], cudaEventDisableTiming));
+        FC_CUDA(cudaEventCreateWithFlags(&randoms_in[i], cudaEventDisableTiming));
+      }
+    } catch (...) {
+      release_streams();
+      throw;
     }
     for (int i = 0; i < slots; ++i) workers.emplace_back([this, i] { worker(i); });
+  }
+
+  void release_streams() {
+    for (auto &x : copy_stream)
+      if (x) cudaStreamDestroy(x), x = nullptr;
+    for (auto &e : data_in)
+      if (e) cudaEventDestroy(e), e = nullptr;
+    for (auto &e : randoms_in)
+      if (e) cudaEventDestroy(e), e = nullptr;
   }
 
   ~Server() {
@@ -196,6 +224,9 @@ struct Server {
     }
     cv_work.notify_all();
     for (auto &t : workers) t.join();
+    for (auto x : copy_stream)
+      if (x) cudaStreamSynchronize(x);
+    release_streams();
   }
 
   uint64_t submit(const fc_job &spec) {
@@ -431,22 +462,44 @@ struct Server {
                                 s.window, s.rmax, s.dr, s.kmax, s.dk, s.maxell,
                                 s.precision);
     Grid *ga = grids[0]->grid.get();
-    const int64_t nmax = max_particles(s);
+    const bool survey = s.kind == FC_SURVEY;
     const size_t cs = std::max(catalog_scratch_bytes(s.data),
-                               s.kind == FC_SURVEY ? catalog_scratch_bytes(s.randoms) : 0);
-    const size_t nbuf = ((size_t)nmax * 32 + 255) / 256 * 256;
-    stage[slot]->resize(std::max<size_t>(nbuf + cs, 32));
-    double *buf = stage[slot]->as<double>();
-    double *scr = reinterpret_cast<double *>(stage[slot]->as<char>() + nbuf);
-    cudaStream_t st = ga->stream;
+                               survey ? catalog_scratch_bytes(s.randoms) : 0);
+    const size_t nbuf_d = stage_rows_bytes(s.data.n);
+    const size_t nbuf_r = survey ? stage_rows_bytes(s.randoms.n) : 0;
+    stage[slot]->resize(std::max<size_t>(nbuf_d + nbuf_r + cs, 32));
+    char *st0 = stage[slot]->as<char>();
+    double *buf_d = reinterpret_cast<double *>(st0);
+    double *buf_r = reinterpret_cast<double *>(st0 + nbuf_d);
+    double *scr = reinterpret_cast<double *>(st0 + nbuf_d + nbuf_r);
+    cudaStream_t cp = copy_stream[slot];
+    // Whatever this job queued is complete when it returns or fails, so the
+    // next job on this worker may reuse the staging and the grids.
+    struct Drain {
+      cudaStream_t s[3];
+      ~Drain() {
+        for (cudaStream_t x : s)
+          if (x) cudaStreamSynchronize(x);
+      }
+    } drain{{cp, ga->stream, survey ? grids[1]->grid->stream : nullptr}};
     lap(7);
+    // Both catalogs come in one after the other on the worker's copy
+    // stream, so the randoms' copy (or generation) runs while the data are
+    // assigned.  (This worker's previous job is complete: its staging is
+    // free.)
+    catalog_generate(s.data, buf_d, cp, scr, cs);
+    FC_CUDA(cudaEventRecord(data_in[slot], cp));
+    if (survey) {
+      catalog_generate(s.randoms, buf_r, cp, scr, cs);
+      FC_CUDA(cudaEventRecord(randoms_in[slot], cp));
+    }
     // Data grid.
     ga->clear();
     assignor_clear(grids[0]->ma);
-    catalog_generate(s.data, buf, st, scr, cs);
-    FC_CUDA(cudaStreamSynchronize(st));
+    FC_CUDA(cudaStreamWaitEvent(ga->stream, data_in[slot], 0));
+    FC_CUDA(cudaEventSynchronize(data_in[slot]));
     lap(0);
-    assignor_add_device(grids[0]->ma, buf, s.data.n);
+    assignor_add_device(grids[0]->ma, buf_d, s.data.n);
     assignor_stats(grids[0]->ma, &j->data_stats);
     lap(1);
     fc_grid *ha = reinterpret_cast<fc_grid *>(ga);
@@ -465,11 +518,10 @@ struct Server {
     Grid *gb = grids[1]->grid.get();
     gb->clear();
     assignor_clear(grids[1]->ma);
-    stream_after(gb->stream, st);
-    catalog_generate(s.randoms, buf, gb->stream, scr, cs);
-    FC_CUDA(cudaStreamSynchronize(gb->stream));
+    FC_CUDA(cudaStreamWaitEvent(gb->stream, randoms_in[slot], 0));
+    FC_CUDA(cudaEventSynchronize(randoms_in[slot]));
     lap(2);
-    assignor_add_device(grids[1]->ma, buf, s.randoms.n);
+    assignor_add_device(grids[1]->ma, buf_r, s.randoms.n);
     assignor_stats(grids[1]->ma, &j->rand_stats);
     lap(3);
     fc_grid *hb = reinterpret_cast<fc_grid *>(gb);
