@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--only-served", action="store_true")
     ap.add_argument("--served-jobs", type=int, default=24)
     ap.add_argument("--served-slots", type=int, default=2)
+    ap.add_argument("--e2e-slots", type=int, default=2)
     ap.add_argument("--mix-jobs", type=int, default=48)
     ap.add_argument("--mix-rate", type=float, default=6.0)
     ap.add_argument("--reference-budget-s", type=float, default=150.0)
@@ -775,7 +776,7 @@ def main():
     res32 = (nn, rr, xi)
     result_bytes = job.result_bytes(nn)
     del job
-    t_e2e = dist.max(run_e2e_served(a, w, D, R, timer))
+    t_e2e = dist.max(run_e2e_served(a, w, D, R, timer, slots=a.e2e_slots))
 
     fp64 = None
     res64 = None
@@ -863,7 +864,7 @@ def main():
                     "h2d_bytes_per_step": int(D.nbytes + R.nbytes),
                     "d2h_bytes_per_step": int(result_bytes),
                     "ms_per_step": 1000.0 * t_e2e / a.steps,
-                    "api": "fftcorr_b200.serve.Server (2 slots), catalogs "
+                    "api": f"fftcorr_b200.serve.Server ({a.e2e_slots} slots), catalogs "
                            "copied from pinned host memory every job, tables "
                            "read back every job"},
             "e2e_sync": {"value": world * a.steps / t_e2e_sync, "unit": "jobs/s",
