@@ -1232,41 +1232,69 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   }
 }
 
-// Weighting of one row's eight pairs of cells for an (ell > 0, m) term, out
-// = Y_lm * in (out may be in), in the form row_poly_form picks (one
-// uniform branch per thread, as in k_zfwd_pp).
-template <int TPC>
-__device__ __forceinline__ void weigh_row(const RowPoly &rp, const YlmParams &p,
-                                          float zt, const float2 *in,
-                                          float2 *out) {
-  auto weigh = [&](auto poly, auto ellc) {
-    constexpr int POLY = decltype(poly)::value, ELL = decltype(ellc)::value;
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const float zu = zt + (float)(2 * TPC * u);
-      const float2 c = in[u];
-      out[u].x = row_weight_form<POLY, ELL>(rp, c.x, zu);
-      out[u].y = row_weight_form<POLY, ELL>(rp, c.y, zu + 1.0f);
-    }
-  };
+// Calls f(POLY, ELL) with the compile-time form of an (ell > 0, m) term's
+// row polynomial (row_poly_form).
+template <typename F>
+__device__ __forceinline__ void with_row_form(const YlmParams &p, F &&f) {
   using std::integral_constant;
   using I2 = integral_constant<int, 2>;
   using I4 = integral_constant<int, 4>;
   if (p.ell == 2) {
     switch (row_poly_form(2, p.m)) {
-      case 0: weigh(integral_constant<int, 0>(), I2()); break;
-      case 1: weigh(integral_constant<int, 1>(), I2()); break;
-      default: weigh(integral_constant<int, 2>(), I2()); break;
+      case 0: f(integral_constant<int, 0>(), I2()); break;
+      case 1: f(integral_constant<int, 1>(), I2()); break;
+      default: f(integral_constant<int, 2>(), I2()); break;
     }
   } else {
     switch (row_poly_form(4, p.m)) {
-      case 0: weigh(integral_constant<int, 0>(), I4()); break;
-      case 1: weigh(integral_constant<int, 1>(), I4()); break;
-      case 2: weigh(integral_constant<int, 2>(), I4()); break;
-      case 3: weigh(integral_constant<int, 3>(), I4()); break;
-      default: weigh(integral_constant<int, 4>(), I4()); break;
+      case 0: f(integral_constant<int, 0>(), I4()); break;
+      case 1: f(integral_constant<int, 1>(), I4()); break;
+      case 2: f(integral_constant<int, 2>(), I4()); break;
+      case 3: f(integral_constant<int, 3>(), I4()); break;
+      default: f(integral_constant<int, 4>(), I4()); break;
     }
   }
+}
+
+// The row polynomial of form POLY at z (z2 = z^2), as row_weight_form.
+template <int POLY>
+__device__ __forceinline__ float row_poly_at(const RowPoly &r, float z, float z2) {
+  if constexpr (POLY == 0) return r.c[0];
+  else if constexpr (POLY == 1) return r.c[1] * z;
+  else if constexpr (POLY == 2) return r.c[2] * z2 + r.c[0];
+  else if constexpr (POLY == 3) return (r.c[3] * z2 + r.c[1]) * z;
+  else return (r.c[4] * z2 + r.c[2]) * z2 + r.c[0];
+}
+
+// One row weighted for two terms a and q: b = Y_q * a, then a = Y_a * a,
+// with the same operations as row_weight_form; z^2 and 1/r^2 depend only
+// on the row and z, so they are computed once for both terms.
+template <int TPC>
+__device__ __forceinline__ void weigh_row_pair(const RowPoly &ra,
+                                               const YlmParams &pa,
+                                               const RowPoly &rq,
+                                               const YlmParams &pq, float zt,
+                                               float2 *a, float2 *b) {
+  with_row_form(pa, [&](auto polya, auto ella) {
+    with_row_form(pq, [&](auto polyq, auto ellq) {
+      constexpr int PA = decltype(polya)::value, EA = decltype(ella)::value;
+      constexpr int PQ = decltype(polyq)::value, EQ = decltype(ellq)::value;
+      auto one = [&](float d, float z, float &wa, float &wq) {
+        const float z2 = z * z;
+        const float ir2 = __fdividef(1.0f, ra.rxy2 + z2 + 1e-20f);
+        const float fa = EA == 2 ? ir2 : ir2 * ir2;
+        const float fq = EQ == 2 ? ir2 : ir2 * ir2;
+        wq = d * row_poly_at<PQ>(rq, z, z2) * fq;
+        wa = d * row_poly_at<PA>(ra, z, z2) * fa;
+      };
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const float zu = zt + (float)(2 * TPC * u);
+        one(a[u].x, zu, a[u].x, b[u].x);
+        one(a[u].y, zu + 1.0f, a[u].y, b[u].y);
+      }
+    });
+  });
 }
 
 // The weighted z pass of two (ell > 0, m) terms at once: thread t of row
@@ -1300,8 +1328,7 @@ __global__ void __launch_bounds__(PP<L>::THREADS)
   float2 a[8], b[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) a[u] = valid ? src[t + Q::TPC * u] : zero;
-  weigh_row<Q::TPC>(rq, pq, zt, a, b);
-  weigh_row<Q::TPC>(ra, pa, zt, a, a);
+  weigh_row_pair<Q::TPC>(ra, pa, rq, pq, zt, a, b);
   CPairS v[8];
 #pragma unroll
   for (int u = 0; u < 8; ++u) v[u] = cpack_s(a[u], b[u]);
