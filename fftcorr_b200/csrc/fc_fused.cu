@@ -1304,7 +1304,7 @@ __device__ __forceinline__ void weigh_row_pair(const RowPoly &ra,
 // the density once instead of twice; the transform and the real-to-complex
 // split are those of k_zfwd_pp.
 template <int L>
-__global__ void __launch_bounds__(PP<L>::THREADS)
+__global__ void __launch_bounds__(PP<L>::THREADS, 1024 / PP<L>::THREADS)
     k_zfwd_pp2(const float *__restrict__ rho, float2 *__restrict__ Wa,
                float2 *__restrict__ Wb, FusedGeom g, YlmParams pa, YlmParams pq,
                double z0, const float2 *__restrict__ tabz,
