@@ -308,6 +308,7 @@ def kernel_profile(job, dD, nD, dR, nR):
 # arrays (profiles/fused_passes_survey512_fp32.md).
 TRAFFIC_PER_LAUNCH_512 = {
     "zfwd": 1048.8e6,
+    "zfwd2": 1603.7e6,
     "yfwd": 1063.2e6,
     "xcorr": 1375.7e6,
     "xcorr00": 801.0e6,
