@@ -302,10 +302,11 @@ def kernel_profile(job, dD, nD, dR, nR):
 
 
 # DRAM bytes (read + write) per launch of the survey pass kernels at 512^3,
-# FP32-mixed, from one ncu capture (dram__bytes.sum.per_second x
-# gpu__time_duration.sum) of `python -m fftcorr_b200.cases survey
-# --precision fp32`, whose passes run on the benchmark's grid and work
-# arrays (profiles/fused_passes_survey512_fp32.md).
+# FP32-mixed, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum,
+# or dram__bytes.sum.per_second x gpu__time_duration.sum) of `python -m
+# fftcorr_b200.cases survey --precision fp32`, one kernel per capture, whose
+# passes run on the benchmark's grid and work arrays (the summaries are
+# kept with the profiles).
 TRAFFIC_PER_LAUNCH_512 = {
     "zfwd": 1048.8e6,
     "zfwd2": 1603.7e6,
