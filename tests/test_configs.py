@@ -167,8 +167,10 @@ def _sector_case(ngrid, nd, nr, kmax, dk):
 
 def _gpu_sector_job(case, precision):
     shape, posmin, cell = case["shape"], case["posmin"], case["cell"]
-    gA = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell)
-    gB = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell)
+    # Grids of the form's precision, as the benchmark job uses them (FP32
+    # cells for the FP32-mixed form).
+    gA = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell, precision=precision)
+    gB = fb.ConfigSpaceGrid.from_geometry(shape, posmin, cell, precision=precision)
     tsc = fb.DistributionScheme.TRIANGULAR_SHAPED_CLOUD
     maA = fb.MassAssignor(gA, tsc, False, 0)
     maB = fb.MassAssignor(gB, tsc, False, 0)
