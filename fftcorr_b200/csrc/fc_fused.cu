@@ -861,54 +861,133 @@ __device__ __forceinline__ void store_pair(float2 *p, const CPair &v, bool v0,
   }
 }
 
-template <int L>
-__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
-    k_yfwd_pp(float2 *__restrict__ W, FusedGeom g,
-              const float2 *__restrict__ taby) {
+// The column pair of thread p in a column pass.  Ordinary CTAs hold
+// adjacent columns c0, c0 + 1 of one plane (one 16-byte access).  When the
+// pass runs with `nyq`, the CTAs of the last column group (SPLIT) instead
+// hold the last column (kz = N2/2, alone in its 16-column group) of planes
+// 2p and 2p + 1 of their group of B planes, so that column does not take a
+// whole group of mostly padding columns per plane.  The kernels branch once
+// per CTA between the two forms, each compiled separately.
+template <bool SPLIT>
+struct ColPair {
+  int64_t b0, b1;  // element offsets of the two columns' first rows
+  bool v0, v1;     // whether each column exists
+  __device__ CPair load(const float2 *a, int64_t row) const {
+    if constexpr (!SPLIT) return load_pair(a + b0 + row);
+    else return cpack(a[b0 + row], a[b1 + row]);
+  }
+  __device__ void store(float2 *a, int64_t row, const CPair &v) const {
+    if constexpr (!SPLIT) {
+      store_pair(a + b0 + row, v, v0, v1);
+    } else {
+      if (v0) a[b0 + row] = clane0(v);
+      if (v1) a[b1 + row] = clane1(v);
+    }
+  }
+  // Asynchronous copy of the pair at `row` into a 16-byte shared slot, laid
+  // out as in memory (re, im of each column).
+  __device__ void copy_async(CPair *slot, const float2 *a, int64_t row) const {
+    if constexpr (!SPLIT) {
+      cp_async16(slot, a + b0 + row);
+    } else {
+      float2 *d = reinterpret_cast<float2 *>(slot);
+      cp_async8(d, a + b0 + row);
+      cp_async8(d + 1, a + b1 + row);
+    }
+  }
+};
+
+// Column pair of thread p in the CTA of group blockIdx.x and plane (or, for
+// SPLIT, plane group) `plane`, in a pass whose `nplanes` planes are `pitch`
+// elements apart.  Returns false when a SPLIT CTA has no planes left.
+template <int B, bool SPLIT>
+__device__ __forceinline__ bool col_pair(ColPair<SPLIT> &c, int p, int plane,
+                                         int64_t pitch, int nplanes,
+                                         const FusedGeom &g) {
+  if constexpr (SPLIT) {
+    const int pl0 = plane * B;
+    if (pl0 >= nplanes) return false;
+    const int pa = pl0 + 2 * p;
+    c.v0 = pa < nplanes;
+    c.v1 = pa + 1 < nplanes;
+    c.b0 = (int64_t)(c.v0 ? pa : 0) * pitch + g.h - 1;
+    c.b1 = (int64_t)(c.v1 ? pa + 1 : 0) * pitch + g.h - 1;
+  } else {
+    const int c0 = blockIdx.x * B + 2 * p;
+    c.v0 = c0 < g.h;
+    c.v1 = c0 + 1 < g.h;
+    c.b0 = (int64_t)plane * pitch + c0;
+    c.b1 = c.b0 + 1;
+  }
+  return true;
+}
+
+// Whether this CTA takes the last column of a group of planes.
+__device__ __forceinline__ bool split_cta(int nyq) {
+  return nyq != 0 && blockIdx.x == gridDim.x - 1;
+}
+
+template <int L, bool SPLIT>
+__device__ __forceinline__ void yfwd_pp_body(float2 *__restrict__ W,
+                                             const FusedGeom &g,
+                                             const float2 *__restrict__ taby) {
   using Q = PY<L>;
   extern __shared__ unsigned char smem_raw[];
   CPair *ex = reinterpret_cast<CPair *>(smem_raw);
   const int t = threadIdx.x / Q::PB;
   const int p = threadIdx.x - t * Q::PB;
-  const int c0 = blockIdx.x * Q::B + 2 * p;
-  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
-  const int64_t base = (int64_t)blockIdx.y * L * g.hp + c0;
+  // Planes are x, L * g.hp elements apart.
+  ColPair<SPLIT> cp;
+  if (!col_pair<Q::B>(cp, p, blockIdx.y, (int64_t)L * g.hp, g.n0, g)) return;
   CPair v[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u)
-    v[u] = load_pair(W + base + (int64_t)(t + Q::TPC * u) * g.hp);
+  for (int u = 0; u < 8; ++u) v[u] = cp.load(W, (int64_t)(t + Q::TPC * u) * g.hp);
   const int rb = Q::rd_base(t, p);
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
              [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, -1);
 #pragma unroll
-  for (int u = 0; u < 8; ++u)
-    store_pair(W + base + (int64_t)(t + Q::TPC * u) * g.hp, v[u], v0, v1);
+  for (int u = 0; u < 8; ++u) cp.store(W, (int64_t)(t + Q::TPC * u) * g.hp, v[u]);
+}
+
+template <int L>
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_yfwd_pp(float2 *__restrict__ W, FusedGeom g,
+              const float2 *__restrict__ taby) {
+  // (Splitting off the last column measured slower here: 194 vs 183 us.)
+  yfwd_pp_body<L, false>(W, g, taby);
 }
 
 // grid2's x transform in the FP32 form: G = DFT_x(W), the same column
 // pairing as the y passes, with rows N1 * hp elements apart.
-template <int L>
-__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
-    k_xfwd_pp(const float2 *__restrict__ W, float2 *__restrict__ G, FusedGeom g,
-              const float2 *__restrict__ tabx) {
+template <int L, bool SPLIT>
+__device__ __forceinline__ void xfwd_pp_body(const float2 *__restrict__ W,
+                                             float2 *__restrict__ G,
+                                             const FusedGeom &g,
+                                             const float2 *__restrict__ tabx) {
   using Q = PY<L>;
   extern __shared__ unsigned char smem_raw[];
   CPair *ex = reinterpret_cast<CPair *>(smem_raw);
   const int t = threadIdx.x / Q::PB;
   const int p = threadIdx.x - t * Q::PB;
-  const int c0 = blockIdx.x * Q::B + 2 * p;
-  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
   const int64_t stride = (int64_t)g.n1 * g.hp;
-  const int64_t base = (int64_t)blockIdx.y * g.hp + c0;
+  // Planes are y, g.hp elements apart.
+  ColPair<SPLIT> cp;
+  if (!col_pair<Q::B>(cp, p, blockIdx.y, g.hp, g.n1, g)) return;
   CPair v[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u) v[u] = load_pair(W + base + (t + Q::TPC * u) * stride);
+  for (int u = 0; u < 8; ++u) v[u] = cp.load(W, (t + Q::TPC * u) * stride);
   const int rb = Q::rd_base(t, p);
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
              [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, tabx, -1);
 #pragma unroll
-  for (int u = 0; u < 8; ++u)
-    store_pair(G + base + (t + Q::TPC * u) * stride, v[u], v0, v1);
+  for (int u = 0; u < 8; ++u) cp.store(G, (t + Q::TPC * u) * stride, v[u]);
+}
+
+template <int L>
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_xfwd_pp(const float2 *__restrict__ W, float2 *__restrict__ G, FusedGeom g,
+              const float2 *__restrict__ tabx) {
+  xfwd_pp_body<L, false>(W, G, g, tabx);
 }
 
 // The FP32 x pass of one (ell, m) term with the same column pairing.
@@ -986,23 +1065,24 @@ __device__ __noinline__ void xcorr_pp_extract(const CPair *ex, int t, int p,
   }
 }
 
-template <int L, int MODE>
-__global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREADS)
-    k_xcorr_pp(const float2 *__restrict__ W, const float2 *__restrict__ G,
-               float2 *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
-               const float2 *__restrict__ tabx, const float *__restrict__ ktab,
-               float w00) {
+template <int L, int MODE, bool SPLIT>
+__device__ __forceinline__ void xcorr_pp_body(
+    const float2 *__restrict__ W, const float2 *__restrict__ G,
+    float2 *__restrict__ out, double *__restrict__ ksub, const FusedGeom &g,
+    const float2 *__restrict__ tabx, const float *__restrict__ ktab, float w00) {
   using Q = PY<L, kXB>;
   extern __shared__ unsigned char smem_raw[];
   CPair *ex = reinterpret_cast<CPair *>(smem_raw);
   const int t = threadIdx.x / Q::PB;
   const int p = threadIdx.x - t * Q::PB;
-  const int cb = blockIdx.x * Q::B;
-  const int c0 = cb + 2 * p;
-  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
   const int yy = blockIdx.y;
   const int64_t stride = (int64_t)g.n1 * g.hp;
-  const int64_t base = (int64_t)yy * g.hp + c0;
+  // Planes are y, g.hp elements apart; with nyq the host has made sure the
+  // last column lies outside the k-subgrid.
+  ColPair<SPLIT> cp;
+  if (!col_pair<Q::B>(cp, p, yy, g.hp, g.n1, g)) return;
+  const int cb = SPLIT ? g.h - 1 : blockIdx.x * Q::B;
+  const int c0 = SPLIT ? g.h - 1 : cb + 2 * p;
   auto exf = [&](int i) { return &ex[Q::row(i) * Q::PB + p]; };
   const int rb = Q::rd_base(t, p);
   auto exr = [&](int u) { return &ex[Q::rd(rb, t, p, u)]; };
@@ -1011,14 +1091,13 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
     const float2 w = f2splat(w00);
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      const CPair q = load_pair(G + base + (t + Q::TPC * u) * stride);
+      const CPair q = cp.load(G, (t + Q::TPC * u) * stride);
       v[u].x = w * __ffma2_rn(q.x, q.x, q.y * q.y);
       v[u].y = f2splat(0.f);
     }
   } else {
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      v[u] = load_pair(W + base + (t + Q::TPC * u) * stride);
+    for (int u = 0; u < 8; ++u) v[u] = cp.load(W, (t + Q::TPC * u) * stride);
     // G's pairs are copied into this thread's own exchange slots while the
     // last pass of the forward transform computes.  A slot then holds the
     // two columns as stored in memory, (re, im) of each, so it is read back
@@ -1026,7 +1105,7 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
     reg_fft<L>(v, t, exf, exr, tabx, -1, 1, [&] {
 #pragma unroll
       for (int u = 0; u < 8; ++u)
-        cp_async16(exr(u), G + base + (t + Q::TPC * u) * stride);
+        cp.copy_async(exr(u), G, (t + Q::TPC * u) * stride);
     });
     cp_async_wait_all();
 #pragma unroll
@@ -1062,7 +1141,7 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
 #pragma unroll
     for (int u = 0; u < 8; u += 7) {
       const int ri = (t + Q::TPC * u + g.ro) & (L - 1);
-      if (ri < g.rs) store_pair(out + base + ri * stride, v[u], v0, v1);
+      if (ri < g.rs) cp.store(out, ri * stride, v[u]);
     }
     return;
   }
@@ -1070,38 +1149,56 @@ __global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREAD
   for (int u = 0; u < 8; ++u) {
     const int x = t + Q::TPC * u;
     for (int ri = (x + g.ro) & (L - 1); ri < g.rs; ri += L)
-      store_pair(out + base + ri * stride, v[u], v0, v1);
+      cp.store(out, ri * stride, v[u]);
   }
 }
 
-template <int L>
-__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
-    k_yinv_pp(const float2 *__restrict__ Wr, float2 *__restrict__ Wry,
-              FusedGeom g, const float2 *__restrict__ taby) {
+template <int L, int MODE>
+__global__ void __launch_bounds__(PY<L, kXB>::THREADS, 1024 / PY<L, kXB>::THREADS)
+    k_xcorr_pp(const float2 *__restrict__ W, const float2 *__restrict__ G,
+               float2 *__restrict__ out, double *__restrict__ ksub, FusedGeom g,
+               const float2 *__restrict__ tabx, const float *__restrict__ ktab,
+               float w00, int nyq) {
+  // The last column split off (nyq) pays in the product mode only; the
+  // ell = 0 mode compiles without it (with it: 215 vs 188 us).
+  if constexpr (MODE == 1) {
+    if (split_cta(nyq)) {
+      xcorr_pp_body<L, MODE, true>(W, G, out, ksub, g, tabx, ktab, w00);
+      return;
+    }
+  }
+  xcorr_pp_body<L, MODE, false>(W, G, out, ksub, g, tabx, ktab, w00);
+}
+
+template <int L, bool SPLIT>
+__device__ __forceinline__ void yinv_pp_body(const float2 *__restrict__ Wr,
+                                             float2 *__restrict__ Wry,
+                                             const FusedGeom &g,
+                                             const float2 *__restrict__ taby) {
   using Q = PY<L>;
   extern __shared__ unsigned char smem_raw[];
   CPair *ex = reinterpret_cast<CPair *>(smem_raw);
   const int t = threadIdx.x / Q::PB;
   const int p = threadIdx.x - t * Q::PB;
-  const int c0 = blockIdx.x * Q::B + 2 * p;
-  const bool v0 = c0 < g.h, v1 = c0 + 1 < g.h;
-  const int ri = blockIdx.y;
-  const int64_t base = (int64_t)ri * L * g.hp + c0;
+  // Planes are the r-subgrid's x rows ri: L * g.hp elements apart in Wr,
+  // rs * g.hp in Wry.
+  ColPair<SPLIT> cp;
+  if (!col_pair<Q::B>(cp, p, blockIdx.y, (int64_t)L * g.hp, g.rs, g)) return;
   CPair v[8];
 #pragma unroll
-  for (int u = 0; u < 8; ++u)
-    v[u] = load_pair(Wr + base + (int64_t)(t + Q::TPC * u) * g.hp);
+  for (int u = 0; u < 8; ++u) v[u] = cp.load(Wr, (int64_t)(t + Q::TPC * u) * g.hp);
   const int rb = Q::rd_base(t, p);
   const bool edges = g.ro <= Q::TPC && g.rs - g.ro <= Q::TPC;  // see k_xcorr_pp
   reg_fft<L>(v, t, [&](int i) { return &ex[Q::row(i) * Q::PB + p]; },
              [&](int u) { return &ex[Q::rd(rb, t, p, u)]; }, taby, +1, 1,
              NoHook{}, edges);
-  const int64_t obase = (int64_t)ri * g.rs * g.hp + c0;
+  ColPair<SPLIT> co;  // the same columns of the same planes in Wry
+  col_pair<Q::B>(co, p, blockIdx.y, (int64_t)g.rs * g.hp, g.rs, g);
   if (edges) {
 #pragma unroll
     for (int u = 0; u < 8; u += 7) {
       const int rj = (t + Q::TPC * u + g.ro) & (L - 1);
-      if (rj < g.rs) store_pair(Wry + obase + (int64_t)rj * g.hp, v[u], v0, v1);
+      if (rj < g.rs) co.store(Wry, (int64_t)rj * g.hp, v[u]);
     }
     return;
   }
@@ -1109,8 +1206,18 @@ __global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
   for (int u = 0; u < 8; ++u) {
     const int y = t + Q::TPC * u;
     for (int rj = (y + g.ro) & (L - 1); rj < g.rs; rj += L)
-      store_pair(Wry + obase + (int64_t)rj * g.hp, v[u], v0, v1);
+      co.store(Wry, (int64_t)rj * g.hp, v[u]);
   }
+}
+
+template <int L>
+__global__ void __launch_bounds__(PY<L>::THREADS, 1024 / PY<L>::THREADS)
+    k_yinv_pp(const float2 *__restrict__ Wr, float2 *__restrict__ Wry,
+              FusedGeom g, const float2 *__restrict__ taby, int nyq) {
+  if (split_cta(nyq))
+    yinv_pp_body<L, true>(Wr, Wry, g, taby);
+  else
+    yinv_pp_body<L, false>(Wr, Wry, g, taby);
 }
 
 // Rows of the z transform, two rows per thread: rows b and b + PB of the
@@ -1755,7 +1862,7 @@ void FusedSurvey::xcorr(bool product, double *ksub, const void *ktab_v,
         dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
         k_xcorr_pp<L, 1><<<gy, Y::THREADS, Y::smem, s>>>(
             W.as<float2>(), G.as<float2>(), Wr.as<float2>(), ksub, g,
-            tabx.as<float2>(), ktab, 0.f);
+            tabx.as<float2>(), ktab, 0.f, nyq_group<Y::B>(ksub != nullptr));
       } else
         k_xcorr_p2<T, L, 1><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
             W.as<C2<T>>(), G.as<C2<T>>(), Wr.as<C2<T>>(), ksub, g,
@@ -1791,7 +1898,7 @@ void FusedSurvey::xcorr00(double *ksub, const void *ktab_v, double w00,
       dim3 gy((g.h + Y::B - 1) / Y::B, g.n1);
       k_xcorr_pp<L, 2><<<gy, Y::THREADS, Y::smem, s>>>(
           nullptr, G.as<float2>(), Wr.as<float2>(), ksub, g, tabx.as<float2>(),
-          ktab, (float)w00);
+          ktab, (float)w00, 0);
     } else {
       dim3 grid((g.h + Q::B - 1) / Q::B, g.n1);
       k_xcorr_p2<T, L, 2><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(
@@ -1811,7 +1918,8 @@ void FusedSurvey::yinv(cudaStream_t s) {
         using Y = PY<L>;
         dim3 grid((g.h + Y::B - 1) / Y::B, g.rs);
         k_yinv_pp<L><<<grid, Y::THREADS, Y::smem, s>>>(
-            Wr.as<float2>(), Wry.as<float2>(), g, taby.as<float2>());
+            Wr.as<float2>(), Wry.as<float2>(), g, taby.as<float2>(),
+            nyq_group<Y::B>(false));
       } else {
         dim3 grid((g.h + Q::B - 1) / Q::B, g.rs);
         k_yinv_p2<T, L><<<grid, Q::THREADS, p2_col_smem<T, L>(), s>>>(

@@ -70,6 +70,13 @@ class FusedSurvey {
   // one launch: term a's result lands in W, term b's in a second buffer
   // that take_second() swaps into W before term b runs with z_done.
   bool pairs() const;
+  // 1 when the last group of B columns holds only the last column (kz =
+  // N2/2), which the paired column passes then take for B planes per CTA;
+  // with k_extract, only when that column lies outside the k-subgrid.
+  template <int B>
+  int nyq_group(bool k_extract) const {
+    return (g.h - 1) % B == 0 && (!k_extract || g.ks2 / 2 < g.h - 1) ? 1 : 0;
+  }
   void zfwd_pair(const void *rho_in, int ell_a, int m_a, int ell_b, int m_b,
                  const double xyz0[3], cudaStream_t s, PhaseHook *hook);
   void take_second() { std::swap(W, W2); }
