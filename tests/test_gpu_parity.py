@@ -349,6 +349,24 @@ def test_cross_correlate_without_grid2_fails():
         c.cross_correlate(np.zeros((16, 16, 16)))
 
 
+@pytest.mark.parametrize("kmax", [0.2, 0.35])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_survey_last_column_group(kmax, precision):
+    """The column passes hand the kz = N2/2 column (alone in its 16-column
+    group) to CTAs that take it for 16 planes each, unless the k-subgrid
+    reaches it: kmax 0.2 keeps it outside, 0.35 (above the Nyquist 0.314)
+    spans every kz.  Both must match the oracle."""
+    shape, cell = (64, 64, 64), 10.0
+    posmin = np.array([-320.0, -320.0, 40.0])
+    nn, _ = _survey_field(shape, cell, posmin, 91)
+    args = (cell, posmin, TSC_ALIASED_CORRECTION, 60.0, 6.0, kmax, 0.03, 4)
+    ref = O.survey_correlate(nn, *args)
+    c = fb.Correlator(shape, *args, precision=precision)
+    c.autocorrelate(nn)
+    _compare_results(c.results(), ref, FP64_RTOL, "last group",
+                     fp32=precision == "fp32")
+
+
 def test_fp32_mixed_within_tolerance(fft_path):
     shape, cell = (48, 48, 48), 12.0
     posmin = np.array([-288.0, -288.0, 30.0])
