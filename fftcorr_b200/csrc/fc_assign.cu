@@ -45,6 +45,9 @@ namespace {
 
 constexpr int kTile = 8;         // tile edge in cells
 constexpr int kTileCells = 512;  // cells per tile
+// A scatter unit with more particles than this is drawn before the others
+// of its colour pass (a quarter of the narrow stencils' staging chunk).
+constexpr uint32_t kHeavyUnit = 128;
 constexpr int kScatterThreads = 256;
 constexpr int kChunk = 256;      // particles staged per shared-memory chunk
 
@@ -276,7 +279,11 @@ __global__ void k_unit_ranges(const uint32_t *__restrict__ units, int64_t nu,
                               unsigned *__restrict__ cnt,
                               uint4 *__restrict__ ranges) {
   // The loop is warp-uniform so that the lanes of a warp that hold
-  // non-empty units of the same colour take their slots with one atomic.
+  // non-empty units of the same colour and class take their slots with one
+  // atomic.  Units of more than kHeavyUnit particles fill the colour's slice
+  // from its end (counter cnt[2 ncolors + c]), the others from its start
+  // (cnt[c]); the scatter draws the heavy ones first, so that no long unit
+  // starts near the end of a pass.
   for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < nu;
        i0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = i0 + threadIdx.x;
@@ -291,15 +298,26 @@ __global__ void k_unit_ranges(const uint32_t *__restrict__ units, int64_t nu,
     const bool ne = i < nu && ts < te;
     const unsigned act = __ballot_sync(0xffffffffu, ne);
     if (!ne) continue;
-    const unsigned grp = __match_any_sync(act, c);
+    const bool heavy = te - ts > kHeavyUnit;
+    const unsigned grp = __match_any_sync(act, 2 * c + (heavy ? 1 : 0));
     const int lane = threadIdx.x & 31;
     const int leader = __ffs(grp) - 1;
+    unsigned *ctr = heavy ? &cnt[2 * ncolors + c] : &cnt[c];
     unsigned base = 0;
-    if (lane == leader) base = atomicAdd(&cnt[c], (unsigned)__popc(grp));
+    if (lane == leader) base = atomicAdd(ctr, (unsigned)__popc(grp));
     base = __shfl_sync(grp, base, leader);
     const unsigned slot = base + (unsigned)__popc(grp & ((1u << lane) - 1u));
-    ranges[coff[c] + slot] = make_uint4(u, ts, te, 0u);
+    const int64_t at = heavy ? coff[c + 1] - 1 - (int64_t)slot : coff[c] + slot;
+    ranges[at] = make_uint4(u, ts, te, 0u);
   }
+}
+
+// Unit i of a colour pass: the heavy units (nh of them, stored from the
+// slice's end backwards) first, then the others from the slice's start.
+__device__ __forceinline__ uint4 pass_unit(const uint4 *__restrict__ front,
+                                           const uint4 *__restrict__ back,
+                                           unsigned nh, unsigned i) {
+  return i < nh ? back[-1 - (int64_t)i] : front[i - nh];
 }
 
 // Exclusive prefix sum over the block (blockDim.x a multiple of 32, at most
@@ -492,8 +510,9 @@ __device__ __forceinline__ size_t foot_cell(int fx, int fy, int fz, int o0,
   return ((size_t)gx * g.n[1] + gy) * g.n[2] + gz;
 }
 
-// ranges: this colour's non-empty units (unit, first, end), `count` of
-// them; `next` is this colour's work counter (zero before the pass).
+// [ranges, ranges_end): this colour's slice of (unit, first, end) records,
+// `count` non-empty units from its start and `count_heavy` heavy ones from
+// its end; `next` is this colour's work counter (zero before the pass).
 // GT is the grid's cell type: each footprint cell's FP64 sum for the unit is
 // added to the cell in FP64 and rounded to GT once.
 template <int S, typename KeyT, int TX, typename GT>
@@ -501,7 +520,9 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
     k_scatter_p(const double *__restrict__ posw, const KeyT *__restrict__ keys,
                 const uint32_t *__restrict__ vals,
                 const uint4 *__restrict__ ranges,
-                const unsigned *__restrict__ count, unsigned *next,
+                const uint4 *__restrict__ ranges_end,
+                const unsigned *__restrict__ count,
+                const unsigned *__restrict__ count_heavy, unsigned *next,
                 AssignGeom g, GT *__restrict__ grid) {
   using Q = ScatterP<S, TX>;
   constexpr int W = Q::W;
@@ -531,11 +552,12 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
 
-  const unsigned n = *count;
+  const unsigned nh = *count_heavy;
+  const unsigned n = *count + nh;
   if (threadIdx.x == 0) {
     const unsigned i0 = atomicAdd(next, 1u);
     s_next = atomicAdd(next, 1u);
-    s_rg = i0 < n ? ranges[i0] : make_uint4(0u, 0u, 0u, 0u);
+    s_rg = i0 < n ? pass_unit(ranges, ranges_end, nh, i0) : make_uint4(0u, 0u, 0u, 0u);
   }
   __syncthreads();
   uint4 rg = s_rg;
@@ -550,7 +572,7 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
     unsigned inn = 0;
     if (threadIdx.x == 0) {
       inn = atomicAdd(next, 1u);
-      if (inext < n) rgn = ranges[inext];
+      if (inext < n) rgn = pass_unit(ranges, ranges_end, nh, inext);
     }
     const uint32_t unit = rg.x, ts = rg.y, te = rg.z;
     const uint32_t tile = unit / NS;
@@ -616,7 +638,6 @@ __global__ void __launch_bounds__(TX * 64, ScatterP<S, TX>::MIN_BLOCKS)
       int lcell[R], lrank[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        const int i = warp * 32 * R + r * 32 + lane;
         // (A key outside this unit cannot occur in a correct sort; it is
         // dropped rather than indexing outside the unit's cells.)
         const KeyT kd = kr[r] - kbase;
@@ -839,7 +860,7 @@ struct Assignor {
   DeviceBuffer color_units;            // units in colour order
   DeviceBuffer unit_ranges;            // uint4 per unit, colour slices
   DeviceBuffer color_off_dev;          // color_offsets on the device
-  DeviceBuffer pass_counters;          // per colour: non-empty units, work
+  DeviceBuffer pass_counters;          // per colour: light units, work, heavy units
   std::vector<int64_t> color_offsets;  // per colour, into color_units
   const void *scatter_fn = nullptr;    // k_scatter_p for this scheme / keys
   size_t scatter_smem_bytes = 0;
@@ -972,7 +993,7 @@ struct Assignor {
     FC_CUDA(cudaMemcpy(color_off_dev.get(), color_offsets.data(),
                        color_offsets.size() * sizeof(int64_t),
                        cudaMemcpyHostToDevice));
-    pass_counters.resize(2 * ncolors * sizeof(unsigned));
+    pass_counters.resize(3 * ncolors * sizeof(unsigned));
   }
 
   size_t key_bytes() const { return wide_keys ? 8 : 4; }
@@ -1211,10 +1232,13 @@ struct Assignor {
       const int64_t nu = color_offsets[c + 1] - color_offsets[c];
       if (nu == 0) continue;
       const uint4 *cr = unit_ranges.as<uint4>() + color_offsets[c];
+      const uint4 *cre = unit_ranges.as<uint4>() + color_offsets[c + 1];
       const unsigned *cnt = counters + c;
+      const unsigned *cnth = counters + 2 * ncolors + c;
       unsigned *nxt = counters + ncolors + c;
-      void *args[] = {(void *)&pw, (void *)&sk, (void *)&sv, (void *)&cr,
-                      (void *)&cnt, (void *)&nxt, (void *)&ga, (void *)&gp};
+      void *args[] = {(void *)&pw, (void *)&sk,  (void *)&sv,  (void *)&cr,
+                      (void *)&cre, (void *)&cnt, (void *)&cnth, (void *)&nxt,
+                      (void *)&ga, (void *)&gp};
       const unsigned ctas = (unsigned)std::min<int64_t>(nu, scatter_ctas);
       FC_CUDA(cudaLaunchKernel(scatter_fn, dim3(ctas), dim3(scatter_threads),
                                args, scatter_smem_bytes, st));
