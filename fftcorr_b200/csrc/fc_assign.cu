@@ -33,6 +33,7 @@
 
 #include "fc_common.cuh"
 #include "fc_internal.h"
+#include "fc_sort.cuh"
 
 #if __has_include("_gen/d12_table.inc")
 #define FC_HAVE_D12 1
@@ -933,6 +934,9 @@ struct Assignor {
           &per_sm, scatter_fn, scatter_threads, scatter_smem_bytes));
       scatter_ctas = (unsigned)std::max(1, per_sm) * (unsigned)sm_count();
     }
+    FC_CUDA(cudaFuncSetAttribute(radix::k_sort_downsweep,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)radix::kDownSmem));
     if (scheme == 2) {
       FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t, double>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1059,8 +1063,7 @@ struct Assignor {
     } else {
       k_keys<uint32_t><<<blocks, 256, 0, stream()>>>(
           src_posw, count, n, geom, (uint32_t)(ntiles * kTileCells),
-          keys.as<uint32_t>(), vals.as<uint32_t>(), parts,
-          counts.as<unsigned long long>());
+          keys.as<uint32_t>(), nullptr, parts, counts.as<unsigned long long>());
     }
     FC_LAUNCH_CHECK();
     k_fold_totals<<<1, 256, 0, stream()>>>(parts, blocks, totals.as<double>());
@@ -1108,7 +1111,7 @@ struct Assignor {
     } else {
       k_keys<uint32_t><<<blocks, 256, 0, stream()>>>(
           src, 0, n, geom, (uint32_t)(ntiles * kTileCells), keys.as<uint32_t>(),
-          vals.as<uint32_t>(), parts, counts.as<unsigned long long>());
+          nullptr, parts, counts.as<unsigned long long>());
     }
     FC_LAUNCH_CHECK();
     k_fold_totals<<<1, 256, 0, stream()>>>(parts, blocks, totals.as<double>());
@@ -1153,22 +1156,86 @@ struct Assignor {
   // [begin_bit, end_bit).  Returns the sorted arrays.
   template <typename KeyT>
   void sort_keys(int begin_bit, const KeyT **sk, const uint32_t **sv) {
+    if constexpr (std::is_same_v<KeyT, uint32_t>) {
+      radix_sort(begin_bit, sk, sv);
+    } else {
+      // Keys wider than 32 bits (grids of more than 2^32 cells).
+      const int64_t n = count;
+      cub::DoubleBuffer<KeyT> dk(keys.as<KeyT>(), keys_alt.as<KeyT>());
+      cub::DoubleBuffer<uint32_t> dv(vals.as<uint32_t>(), vals_alt.as<uint32_t>());
+      size_t temp = 0;
+      FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, n, begin_bit,
+                                              end_bit, stream()));
+      if (graph_mode)
+        FC_REQUIRE(temp <= cub_temp.bytes(), FC_ERR_STATE,
+                   "sort scratch was not prepared for this many particles");
+      cub_temp.resize(temp);
+      if (!graph_mode) sort_timer.start(stream());
+      FC_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp.get(), temp, dk, dv, n,
+                                              begin_bit, end_bit, stream()));
+      if (!graph_mode) sort_timer.stop(stream());
+      *sk = dk.Current();
+      *sv = dv.Current();
+    }
+  }
+
+  // The key of particles outside the grid, and the bits of the valid keys
+  // (the invalid key sorts last through a digit of its own).
+  uint32_t invalid_key32() const { return (uint32_t)(ntiles * kTileCells); }
+  int valid_end_bit() const {
+    const uint64_t max_valid = (uint64_t)invalid_key32() - 1;
+    int e = 1;
+    while (e < 32 && (max_valid >> e) != 0) ++e;
+    return e;
+  }
+
+  // Scratch of the 32-bit-key sort for n particles, either sort range.
+  size_t radix_scratch(int64_t n) const {
+    return std::max(radix::sort_plan(n, 0, valid_end_bit()).scratch_bytes(),
+                    radix::sort_plan(n, unit_shift, valid_end_bit()).scratch_bytes());
+  }
+
+  // The stable LSD radix sort of the 32-bit keys (fc_sort.cuh): the first
+  // pass reads the keys in place with implicit indices, later passes
+  // alternate between the two key and index buffers.
+  void radix_sort(int begin_bit, const uint32_t **sk, const uint32_t **sv) {
+    using namespace radix;
     const int64_t n = count;
-    cub::DoubleBuffer<KeyT> dk(keys.as<KeyT>(), keys_alt.as<KeyT>());
-    cub::DoubleBuffer<uint32_t> dv(vals.as<uint32_t>(), vals_alt.as<uint32_t>());
-    size_t temp = 0;
-    FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, n, begin_bit,
-                                            end_bit, stream()));
+    const SortPlan p = sort_plan(n, begin_bit, valid_end_bit());
+    const uint32_t invalid = invalid_key32();
     if (graph_mode)
-      FC_REQUIRE(temp <= cub_temp.bytes(), FC_ERR_STATE,
+      FC_REQUIRE(p.scratch_bytes() <= cub_temp.bytes(), FC_ERR_STATE,
                  "sort scratch was not prepared for this many particles");
-    cub_temp.resize(temp);
-    if (!graph_mode) sort_timer.start(stream());
-    FC_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp.get(), temp, dk, dv, n,
-                                            begin_bit, end_bit, stream()));
-    if (!graph_mode) sort_timer.stop(stream());
-    *sk = dk.Current();
-    *sv = dv.Current();
+    cub_temp.resize(p.scratch_bytes());
+    uint32_t *cnt = cub_temp.as<uint32_t>();
+    uint32_t *sums = cnt + p.m;
+    cudaStream_t st = stream();
+    if (!graph_mode) sort_timer.start(st);
+    const uint32_t *kin = keys.as<uint32_t>();
+    const uint32_t *vin = nullptr;
+    uint32_t *kbuf[2] = {keys_alt.as<uint32_t>(), keys.as<uint32_t>()};
+    uint32_t *vbuf[2] = {vals_alt.as<uint32_t>(), vals.as<uint32_t>()};
+    for (int pass = 0; pass < p.passes; ++pass) {
+      const int shift = begin_bit + pass * p.bits;
+      k_sort_upsweep<<<(unsigned)p.ntiles, kSortThreads, 0, st>>>(
+          kin, n, invalid, shift, p.bits, p.ntiles, cnt);
+      FC_LAUNCH_CHECK();
+      k_sort_scan_reduce<<<(unsigned)p.nchunks, kSortThreads, 0, st>>>(cnt, p.m, sums);
+      FC_LAUNCH_CHECK();
+      k_sort_scan_top<<<1, kSortThreads, 0, st>>>(sums, p.nchunks);
+      FC_LAUNCH_CHECK();
+      k_sort_scan_apply<<<(unsigned)p.nchunks, kSortThreads, 0, st>>>(cnt, p.m, sums);
+      FC_LAUNCH_CHECK();
+      uint32_t *kout = kbuf[pass & 1], *vout = vbuf[pass & 1];
+      k_sort_downsweep<<<(unsigned)p.ntiles, kSortThreads, kDownSmem, st>>>(
+          kin, vin, n, invalid, shift, p.bits, p.ntiles, cnt, kout, vout);
+      FC_LAUNCH_CHECK();
+      kin = kout;
+      vin = vout;
+    }
+    if (!graph_mode) sort_timer.stop(st);
+    *sk = kin;
+    *sv = vin;
   }
 
   // D12: sort by cell key, then the tile scatter.
@@ -1283,10 +1350,7 @@ struct Assignor {
       FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, max_n, 0,
                                               end_bit, stream()));
     } else {
-      cub::DoubleBuffer<uint32_t> dk(keys.as<uint32_t>(), keys_alt.as<uint32_t>());
-      cub::DoubleBuffer<uint32_t> dv(vals.as<uint32_t>(), vals_alt.as<uint32_t>());
-      FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, max_n, 0,
-                                              end_bit, stream()));
+      temp = radix_scratch(std::max<int64_t>(max_n, 1));
     }
     cub_temp.resize(temp + 1024);
   }
