@@ -934,9 +934,10 @@ struct Assignor {
           &per_sm, scatter_fn, scatter_threads, scatter_smem_bytes));
       scatter_ctas = (unsigned)std::max(1, per_sm) * (unsigned)sm_count();
     }
-    FC_CUDA(cudaFuncSetAttribute(radix::k_sort_downsweep,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)radix::kDownSmem));
+    for (int b = 1; b <= radix::kMaxBits; ++b)
+      FC_CUDA(cudaFuncSetAttribute(radix::downsweep_kernel(b),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)radix::kDownSmem));
     if (scheme == 2) {
       FC_CUDA(cudaFuncSetAttribute(k_scatter<2, uint32_t, double>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1227,8 +1228,8 @@ struct Assignor {
       k_sort_scan_apply<<<(unsigned)p.nchunks, kSortThreads, 0, st>>>(cnt, p.m, sums);
       FC_LAUNCH_CHECK();
       uint32_t *kout = kbuf[pass & 1], *vout = vbuf[pass & 1];
-      k_sort_downsweep<<<(unsigned)p.ntiles, kSortThreads, kDownSmem, st>>>(
-          kin, vin, n, invalid, shift, p.bits, p.ntiles, cnt, kout, vout);
+      downsweep_kernel(p.bits)<<<(unsigned)p.ntiles, kSortThreads, kDownSmem, st>>>(
+          kin, vin, n, invalid, shift, p.ntiles, cnt, kout, vout);
       FC_LAUNCH_CHECK();
       kin = kout;
       vin = vout;

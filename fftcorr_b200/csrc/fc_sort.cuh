@@ -212,11 +212,12 @@ __global__ void __launch_bounds__(kSortThreads)
 
 // Downsweep: tile blockIdx.x's keys (and values; implicit indices when
 // vals_in is null) to their stable sorted positions by sort_digit.  off is
-// the scanned count matrix.
+// the scanned count matrix.  BITS is the pass's digit width.
+template <int BITS>
 __global__ void __launch_bounds__(kSortThreads, 2)
     k_sort_downsweep(const uint32_t *__restrict__ keys_in,
                      const uint32_t *__restrict__ vals_in, int64_t n,
-                     uint32_t invalid, int shift, int bits, int64_t ntiles,
+                     uint32_t invalid, int shift, int64_t ntiles,
                      const uint32_t *__restrict__ off,
                      uint32_t *__restrict__ keys_out,
                      uint32_t *__restrict__ vals_out) {
@@ -228,9 +229,9 @@ __global__ void __launch_bounds__(kSortThreads, 2)
   uint32_t *skeys = gstart + kBinsCap;                // [kSortTile]
   uint32_t *svals = skeys + kSortTile;                // [kSortTile]
   __shared__ uint32_t sh[32];
-  const int bins = 1 << bits;
-  const int nd = bins + 1;
-  const uint32_t mask = (uint32_t)bins - 1u;
+  constexpr int bins = 1 << BITS;
+  constexpr int nd = bins + 1;
+  constexpr uint32_t mask = (uint32_t)bins - 1u;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   const int64_t t = blockIdx.x;
@@ -254,13 +255,13 @@ __global__ void __launch_bounds__(kSortThreads, 2)
     const int i = wbase + r * 32 + lane;
     const bool valid = i < cnt_tile;
     const uint32_t d = valid ? sort_digit(k[r], invalid, shift, mask) : 0u;
-    // Lanes holding the same digit: bits 0 .. bits of d (bit `bits` marks
+    // Lanes holding the same digit: bits 0 .. BITS of d (bit BITS marks
     // the invalid keys' digit), one ballot each.
     unsigned peers = __ballot_sync(0xffffffffu, valid);
-    for (int q = 0; q <= bits; ++q) {
+#pragma unroll
+    for (int q = 0; q <= BITS; ++q) {
       const unsigned bit = (d >> q) & 1u;
-      const unsigned m = __ballot_sync(0xffffffffu, bit);
-      peers &= bit ? m : ~m;
+      peers &= __ballot_sync(0xffffffffu, bit) ^ (bit - 1u);
     }
     const int leader = valid ? __ffs(peers) - 1 : lane;
     uint32_t b = 0;
@@ -332,6 +333,28 @@ __global__ void __launch_bounds__(kSortThreads, 2)
     vals_out[gp] = svals[i];
   }
 }
+
+using DownsweepFn = void (*)(const uint32_t *, const uint32_t *, int64_t,
+                             uint32_t, int, int64_t, const uint32_t *,
+                             uint32_t *, uint32_t *);
+
+// The downsweep for a digit width of 1 .. kMaxBits bits.
+inline DownsweepFn downsweep_kernel(int bits) {
+  switch (bits) {
+    case 1: return k_sort_downsweep<1>;
+    case 2: return k_sort_downsweep<2>;
+    case 3: return k_sort_downsweep<3>;
+    case 4: return k_sort_downsweep<4>;
+    case 5: return k_sort_downsweep<5>;
+    case 6: return k_sort_downsweep<6>;
+    case 7: return k_sort_downsweep<7>;
+    case 8: return k_sort_downsweep<8>;
+    case 9: return k_sort_downsweep<9>;
+    case 10: return k_sort_downsweep<10>;
+    default: return nullptr;
+  }
+}
+static_assert(kMaxBits == 10, "one downsweep instance per digit width");
 
 }  // namespace radix
 }  // namespace fc
