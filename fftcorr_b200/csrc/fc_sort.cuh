@@ -1,9 +1,9 @@
 // Stable LSD radix sort of 32-bit keys with 32-bit values, for the
-// particle sort of mass assignment (the reference sorts nothing: its
-// MassAssignor scatters particles in input order, mass_assignor.h:127-191;
-// the sort here orders the scatter by unit, and a stable sort keeps each
-// cell's particles in input order, so the grid is the same bits on every
-// run).
+// particle sort of mass assignment.  The reference's MassAssignor merge-sorts
+// each buffer of particles by x before its slab-parallel scatter
+// (cc/particle_mesh/mass_assignor.h:137-148, merge_sort_omp.h); here the
+// particles are ordered by scatter unit, and a stable sort keeps each cell's
+// particles in input order, so the grid is the same bits on every run.
 //
 // Each pass sorts by one digit of up to kMaxBits bits in three steps, with
 // no inter-block waits:
