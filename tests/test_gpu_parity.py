@@ -94,6 +94,37 @@ def test_mass_assign_matches_oracle(scheme, periodic, shape):
 
 
 @pytest.mark.parametrize("scheme", [1, 2])
+@pytest.mark.parametrize("n", [1, 8191, 8192, 8193, 24581])
+def test_particle_sort_tiles_and_skipped_particles(scheme, n):
+    """The particle sort's edge cases: counts around its 8192-key tiles,
+    about two thirds of the particles outside the grid (their keys sort last in
+    a digit of their own), and a grid of 576 tiles, so that the unit bits
+    (TSC) and the full cell keys (D12) both take two passes."""
+    shape, cell = (64, 64, 72), 4.0
+    posmin = np.array([1.0, -2.0, 50.0])
+    box = np.array(shape) * cell
+    posw = uniform_catalog(n, posmin - 0.2 * box, posmin + 1.2 * box, 100 + n,
+                           weights="random")
+    g, ma = _assign_gpu(posw, shape, posmin, cell, scheme, False)
+    ref, st = O.mass_assign(posw, shape, posmin, cell, scheme, False)
+    got = _device_grid_values(g)
+    assert np.max(np.abs(got - ref)) <= 1e-12 * max(np.max(np.abs(ref)), 1e-300)
+    assert ma.num_added == int(st[0])
+    assert ma.num_skipped == int(st[1])
+
+
+@pytest.mark.parametrize("scheme", [1, 2])
+def test_every_particle_outside_the_grid(scheme):
+    shape, cell = (16, 16, 16), 10.0
+    posmin = np.zeros(3)
+    posw = uniform_catalog(10000, [200.0, 0.0, 0.0], [300.0, 160.0, 160.0], 5,
+                           weights="random")
+    g, ma = _assign_gpu(posw, shape, posmin, cell, scheme, False)
+    assert ma.num_added == 0 and ma.num_skipped == 10000
+    assert not np.any(_device_grid_values(g))
+
+
+@pytest.mark.parametrize("scheme", [1, 2])
 def test_tiny_periodic_grid_wraps_onto_itself(scheme):
     # Stencils wider than the grid (test_mass_assignor.py uses a 2^3 grid).
     shape = (2, 3, 2)
