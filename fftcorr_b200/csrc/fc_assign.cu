@@ -853,7 +853,7 @@ struct Assignor {
   // Buffered particles.
   int64_t count = 0;
   int64_t capacity = 0;
-  DeviceBuffer posw, keys, keys_alt, vals, vals_alt, cub_temp;
+  DeviceBuffer posw, keys, keys_alt, vals, vals_alt, sort_temp;
   // NGP/CIC/TSC sort by unit only (key bits from unit_shift up): the
   // scatter orders each unit's particles by cell itself.
   int unit_shift = 0;
@@ -1036,8 +1036,11 @@ struct Assignor {
                               cudaMemcpyDeviceToDevice, stream()));
       FC_CUDA(cudaMemcpyAsync(nk.get(), keys.get(), count * key_bytes(),
                               cudaMemcpyDeviceToDevice, stream()));
-      FC_CUDA(cudaMemcpyAsync(nv.get(), vals.get(), count * sizeof(uint32_t),
-                              cudaMemcpyDeviceToDevice, stream()));
+      // Only wide keys keep an index array before the sort (the 32-bit
+      // sort's first pass takes each key's position as its index).
+      if (wide_keys)
+        FC_CUDA(cudaMemcpyAsync(nv.get(), vals.get(), count * sizeof(uint32_t),
+                                cudaMemcpyDeviceToDevice, stream()));
       FC_CUDA(cudaStreamSynchronize(stream()));
     }
     posw = std::move(np);
@@ -1168,11 +1171,11 @@ struct Assignor {
       FC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, dk, dv, n, begin_bit,
                                               end_bit, stream()));
       if (graph_mode)
-        FC_REQUIRE(temp <= cub_temp.bytes(), FC_ERR_STATE,
+        FC_REQUIRE(temp <= sort_temp.bytes(), FC_ERR_STATE,
                    "sort scratch was not prepared for this many particles");
-      cub_temp.resize(temp);
+      sort_temp.resize(temp);
       if (!graph_mode) sort_timer.start(stream());
-      FC_CUDA(cub::DeviceRadixSort::SortPairs(cub_temp.get(), temp, dk, dv, n,
+      FC_CUDA(cub::DeviceRadixSort::SortPairs(sort_temp.get(), temp, dk, dv, n,
                                               begin_bit, end_bit, stream()));
       if (!graph_mode) sort_timer.stop(stream());
       *sk = dk.Current();
@@ -1205,10 +1208,10 @@ struct Assignor {
     const SortPlan p = sort_plan(n, begin_bit, valid_end_bit());
     const uint32_t invalid = invalid_key32();
     if (graph_mode)
-      FC_REQUIRE(p.scratch_bytes() <= cub_temp.bytes(), FC_ERR_STATE,
+      FC_REQUIRE(p.scratch_bytes() <= sort_temp.bytes(), FC_ERR_STATE,
                  "sort scratch was not prepared for this many particles");
-    cub_temp.resize(p.scratch_bytes());
-    uint32_t *cnt = cub_temp.as<uint32_t>();
+    sort_temp.resize(p.scratch_bytes());
+    uint32_t *cnt = sort_temp.as<uint32_t>();
     uint32_t *sums = cnt + p.m;
     cudaStream_t st = stream();
     if (!graph_mode) sort_timer.start(st);
@@ -1353,7 +1356,7 @@ struct Assignor {
     } else {
       temp = radix_scratch(std::max<int64_t>(max_n, 1));
     }
-    cub_temp.resize(temp + 1024);
+    sort_temp.resize(temp + 1024);
   }
 
   // Batched form: clear the running totals and assign n particles from a
