@@ -113,6 +113,43 @@ def test_particle_sort_tiles_and_skipped_particles(scheme, n):
     assert ma.num_skipped == int(st[1])
 
 
+@pytest.mark.parametrize("scheme", [0, 1, 3])
+def test_cell_sums_follow_input_order(scheme):
+    """Bit-level check that each cell sums its particles in input order
+    (stable sort, ordered ranking in the scatter).  Three particles at one
+    cell centre carry weights whose FP64 sum depends on the order: with
+    [1, 2^-60, -1] only orders that leave 2^-60 last give a nonzero cell,
+    and with [1, -1, 2^-60] every order but those ending in 2^-60 gives 0
+    where input order gives exactly c 2^-60 (c the stencil's product, a
+    product of 1/8, 1/2 and 3/4, so every term is exact).  The three are
+    spread over different 8192-key sort tiles among 30000 other particles
+    whose footprints do not reach them."""
+    t = 2.0 ** -60
+    shape, cell = (32, 32, 32), 1.0
+    rng = np.random.default_rng(23)
+    posw = np.empty((30000, 4))
+    posw[:, 0] = rng.uniform(14.0, 30.0, 30000)
+    posw[:, 1:3] = rng.uniform(0.0, 32.0, (30000, 2))
+    posw[:, 3] = rng.uniform(0.5, 1.5, 30000)
+    a_idx, b_idx = (5, 15000, 29000), (7, 15002, 29002)
+    for i, w in zip(a_idx, (1.0, t, -1.0)):
+        posw[i] = (5.5, 5.5, 5.5, w)
+    for i, w in zip(b_idx, (1.0, -1.0, t)):
+        posw[i] = (5.5, 5.5, 20.5, w)
+    g, ma = _assign_gpu(posw, shape, np.zeros(3), cell, scheme, False)
+    got = _device_grid_values(g)
+    # Stencil weights at a cell centre and their offsets from the home cell.
+    wts, off = {0: ([1.0], [0]), 1: ([0.125, 0.75, 0.125], [-1, 0, 1]),
+                3: ([0.5, 0.5], [0, 1])}[scheme]
+    want = np.zeros(shape)
+    for ax, wx in zip(off, wts):
+        for ay, wy in zip(off, wts):
+            for az, wz in zip(off, wts):
+                want[5 + ax, 5 + ay, 20 + az] = wx * wy * wz * t
+    np.testing.assert_array_equal(got[:12], want[:12])
+    assert ma.num_added == 30000
+
+
 @pytest.mark.parametrize("scheme", [1, 2])
 def test_every_particle_outside_the_grid(scheme):
     shape, cell = (16, 16, 16), 10.0
