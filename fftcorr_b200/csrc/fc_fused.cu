@@ -425,8 +425,6 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 ? 3 : 2))
     const int rk = idx - b * g.rs;
     const int row = row0 + b;
     if (row >= nrows) continue;
-    const int ri = row / g.rs;
-    const int rj = row - ri * g.rs;
     const int z = ((rk - g.ro) % g.n2 + g.n2) % g.n2;
     const C zz = buf[(z >> 1) * BP + b];
     const double v = (double)((z & 1) ? zz.y : zz.x);
@@ -444,7 +442,6 @@ struct P2 {
   static constexpr int B = (Tile<T>::B < 8192 / L) ? Tile<T>::B : 8192 / L;
   static constexpr int TPC = L / 8;
   static constexpr int THREADS = TPC * B;
-  static constexpr int BP = B + 1;
   // Exchange rows of B elements: a 128-byte shared-memory line holds R of
   // them.  Row i is stored at row i ^ ((i >> 3) & (R - 1)), which spreads
   // the rows a warp touches in every Stockham write and read evenly over
@@ -774,8 +771,6 @@ __global__ void __launch_bounds__(P2<T, L>::THREADS)
   auto exf = [&](int i) { return &ex[b * RP + i + (i >> 3)]; };
   reg_fft<L>(v, t, exf, tabz, +1, 2);
   if (!valid) return;
-  const int ri = row / g.rs;
-  const int rj = row - ri * g.rs;
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int jj = t + Q::TPC * u;
